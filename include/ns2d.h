@@ -1,0 +1,197 @@
+/*
+ * include/ns2d.h -- C ABI of libns2d.so, the B200 (sm_100a) pseudospectral
+ * time step of the 2-D vorticity Navier-Stokes solver.
+ *
+ * The entry points replace the reference solver's FFTW-MPI path
+ * (EndCar808/2D-Navier-Stokes, Solver/src).  Each declaration names the
+ * reference function it stands in for.  The arrays that cross this boundary use
+ * the reference's own layouts:
+ *
+ *   spectral field  : [nx][ny/2+1] complex128, interleaved (re, im) doubles,
+ *                     row i <-> kx = i (i <= nx/2) or i - nx, column j <-> ky = j
+ *                     (Solver/src/solver.c:2042-2066); the state "w_hat".
+ *   real field      : [nx][ny] float64 (unpadded; the reference pads rows to
+ *                     ny+2 for FFTW in place, which is a storage detail).
+ *
+ * All functions return an ns2d_status; NS2D_OK is 0.  The reference exits the
+ * process on every failure (Solver/src/solver.c:2314-2325, :2643-2651); here
+ * the error is returned and a message is kept per handle (ns2d_last_error).
+ * A handle is not thread-safe; distinct handles are independent.  All state is
+ * device resident; host pointers are copied in and out within the call.
+ */
+#ifndef NS2D_H
+#define NS2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NS2D_ABI_VERSION 1
+
+typedef enum ns2d_status {
+    NS2D_OK = 0,
+    NS2D_ERR_INVALID = 1,     /* bad argument or parameter combination            */
+    NS2D_ERR_UNSUPPORTED = 2, /* valid in the reference, not built here (e.g. N)  */
+    NS2D_ERR_CUDA = 3,        /* CUDA runtime error (message in ns2d_last_error)  */
+    NS2D_ERR_NOMEM = 4,       /* device or host allocation failed                 */
+    NS2D_ERR_BLOWUP = 5,      /* max|w| >= 1e100 or non-finite (SystemCheck)      */
+    NS2D_ERR_DT = 6,          /* dt <= 1e-10 (SystemCheck)                        */
+    NS2D_ERR_ITERS = 7,       /* iteration limit 1e12 reached (SystemCheck)       */
+    NS2D_ERR_STATE = 8,       /* call out of order (e.g. AB4 history missing)     */
+    NS2D_ERR_NO_DEVICE = 9    /* no CUDA device / extension not usable            */
+} ns2d_status;
+
+/* Compile-time switches of Solver/src/data_types.h:49-61 and Solver/Makefile:55-67,
+   selectable per handle. */
+typedef enum ns2d_system { NS2D_NAVIER = 0, NS2D_EULER = 1 } ns2d_system;
+typedef enum ns2d_integrator {
+    NS2D_RK4CN = 0, /* __RK4CN: RK4 with Crank-Nicolson linear term (stock)  */
+    NS2D_RK4 = 1,   /* __RK4  : explicit RK4                                  */
+    NS2D_AB4 = 2,   /* __AB4  : AB4 + CN after three RK4CN start-up steps     */
+    NS2D_DP5 = 3    /* __DPRK5: Dormand-Prince 5(4) with step-size control    */
+} ns2d_integrator;
+typedef enum ns2d_dealias { NS2D_DEALIAS_23 = 0, NS2D_DEALIAS_HOU_LI = 1 } ns2d_dealias;
+typedef enum ns2d_forcing {
+    NS2D_FORCING_NONE = 0,
+    NS2D_FORCING_KOLM = 1, /* "KOLM": one mode (kx=0, ky=force_k), value -F*n/2 */
+    NS2D_FORCING_ZERO = 2  /* "ZERO": listed modes set to 0 each step          */
+} ns2d_forcing;
+typedef enum ns2d_precision { NS2D_FP64 = 0, NS2D_FP32 = 1 } ns2d_precision;
+
+/* Reference behaviours that differ from the textbook scheme.  Setting the bit
+   reproduces the reference exactly; clearing it gives the corrected form. */
+enum {
+    NS2D_QUIRK_CONJ_STATE = 1 << 0,  /* ForceConjugacy writes the *state* from the RHS input (solver.c:1031,2096-2103) */
+    NS2D_QUIRK_HYPER_LATCH = 1 << 1, /* `=` for `==` in the viscous branches latches hyperviscosity on (solver.c:675,843) */
+    NS2D_QUIRK_RK4_LINEAR = 1 << 2,  /* explicit RK4 adds +dt*D*X to each stage (solver.c:664-684)                     */
+    NS2D_QUIRK_HOU_LI_INT = 1 << 3,  /* Hou-Li filter with integer k/(N/2) (solver.c:1088)                            */
+    NS2D_QUIRK_CFL_INDEX = 1 << 4,   /* CFL velocity with row index (i*Ny)/2+1 (solver.c:2394)                        */
+    NS2D_QUIRK_ENST_DISS = 1 << 5,   /* enstrophy dissipation weight-2 branch without pre_fac (sys_msr.c:225)          */
+    NS2D_QUIRKS_REFERENCE = 0x3f
+};
+
+typedef struct ns2d_params {
+    int32_t nx, ny;           /* grid; powers of two, 16..2048 (reference: -n -n)       */
+    int32_t system;           /* ns2d_system                                           */
+    int32_t integrator;       /* ns2d_integrator                                       */
+    int32_t dealias;          /* ns2d_dealias                                          */
+    int32_t forcing;          /* ns2d_forcing                                          */
+    int32_t force_k;          /* -f 2nd                                                */
+    int32_t quirks;           /* NS2D_QUIRK_* bits                                     */
+    double force_scale;       /* -f 3rd                                                */
+    double nu;                /* -v 1st                                                */
+    double hyper_visc_pow;    /* -v 3rd                                                */
+    double ekmn_alpha;        /* -d 1st                                                */
+    double ekmn_drag_pow;     /* -d 3rd                                                */
+    int32_t hyper_visc_flag;  /* -v 2nd                                                */
+    int32_t ekmn_drag_flag;   /* -d 2nd                                                */
+    int32_t adapt_step_flag;  /* -h 2nd                                                */
+    int32_t cfl_cond_flag;    /* -c 1st                                                */
+    double cfl_const;         /* -c 2nd                                                */
+    double dt;                /* -h 1st: initial / fixed step                          */
+    int32_t precision;        /* ns2d_precision                                        */
+    int32_t flux_diagnostics; /* 1 = the stock dataset flags (__ENST_FLUX...): the
+                                 measurables call evaluates the RHS of the state     */
+    int32_t device;           /* CUDA device ordinal                                  */
+    int32_t reserved;
+} ns2d_params;
+
+/* Scalars of ComputeSystemMeasurables (Solver/src/sys_msr.c:32-373), in order. */
+typedef struct ns2d_measures {
+    double energy, enstrophy, palinstrophy, forcing_input, divergence;
+    double energy_diss, enstrophy_diss;
+    double d_enrg_dt_sbst, enrg_flux_sbst, enrg_diss_sbst;
+    double d_enst_dt_sbst, enst_flux_sbst, enst_diss_sbst;
+} ns2d_measures;
+
+/* What GetMaxData (Solver/src/solver.c:2171) reduces. */
+typedef enum ns2d_max_kind { NS2D_MAX_VORT = 0, NS2D_MAX_VEL = 1, NS2D_MAX_VORT_FOUR = 2 } ns2d_max_kind;
+
+typedef struct ns2d_handle ns2d_handle;
+
+/* Defaults of GetCMLArgs (Solver/src/utils.c:51-90) plus the stock compile
+   switches: 64x64, nu = 1e-4, dt = 1e-4, RK4CN, 2/3 dealias, no forcing,
+   flux diagnostics on, all reference quirks on, FP64. */
+ns2d_status ns2d_params_default(ns2d_params* p);
+
+ns2d_status ns2d_create(const ns2d_params* p, ns2d_handle** out);
+ns2d_status ns2d_destroy(ns2d_handle* h);
+const char* ns2d_last_error(const ns2d_handle* h);
+const char* ns2d_status_string(ns2d_status s);
+int ns2d_abi_version(void);
+
+/* Sizes: ny/2+1 and the spectrum bin count n_spect (sys_msr.c:394). */
+ns2d_status ns2d_dims(const ns2d_handle* h, int32_t* nx, int32_t* ny, int32_t* nyf, int32_t* n_spect);
+
+/* State in/out (reference layout, host memory).  Stand-in for the reference's
+   direct use of run_data->w_hat after InitialConditions (solver.c:89). */
+ns2d_status ns2d_set_w_hat(ns2d_handle* h, const double* w_hat);
+ns2d_status ns2d_get_w_hat(ns2d_handle* h, double* w_hat);
+/* Same, with device pointers (no host copy). */
+ns2d_status ns2d_set_w_hat_device(ns2d_handle* h, const double* d_w_hat);
+ns2d_status ns2d_get_w_hat_device(ns2d_handle* h, double* d_w_hat);
+
+/* ComputeForcing (Solver/src/force.c:516): forcing values for this step. */
+ns2d_status ns2d_compute_forcing(ns2d_handle* h, double dt);
+
+/* NonlinearRHSBatch (Solver/src/solver.c:884; solver.h:39).  in == NULL means
+   the state itself (stage-1 form).  out receives the dealiased nonlinear term
+   plus forcing.  With NS2D_QUIRK_CONJ_STATE the state's ky = 0, kx < 0 entries
+   are overwritten with conj(in[|kx|, 0]) exactly as the reference does. */
+ns2d_status ns2d_nonlinear_rhs(ns2d_handle* h, const double* in, double* out);
+
+/* RK4Step (Solver/src/solver.c:625; solver.h:26), RK4CN or RK4 per params. */
+ns2d_status ns2d_rk4_step(ns2d_handle* h, double dt);
+
+/* AB4Step (Solver/src/solver.c:261; solver.h:30).  iters is the reference's
+   1-based iteration counter: iters <= 3 take RK4CN start-up steps. */
+ns2d_status ns2d_ab4_step(ns2d_handle* h, double dt, int32_t iters);
+
+/* nsteps fixed-dt steps of the configured integrator without host round trips
+   (the loop body of SpectralSolve, solver.c:142-236, minus saving). */
+ns2d_status ns2d_step_n(ns2d_handle* h, int32_t nsteps, double dt);
+
+/* ApplyDealiasing (solver.c:1039) on a host array of array_dim interleaved
+   spectral fields, in place. */
+ns2d_status ns2d_apply_dealiasing(ns2d_handle* h, double* arr, int32_t array_dim);
+
+/* ForceConjugacy (solver.c:2074): state[kx<0, 0] = conj(arr[|kx|, 0]).
+   arr == NULL means the state itself. */
+ns2d_status ns2d_force_conjugacy(ns2d_handle* h, const double* arr);
+
+/* GetMaxData (solver.c:2171). */
+ns2d_status ns2d_get_max_data(ns2d_handle* h, int32_t kind, double* out);
+
+/* GetTimestep (solver.c:2376): CFL or vorticity-ratio adaptive step; updates
+   the handle's min/max dt record. */
+ns2d_status ns2d_get_timestep(ns2d_handle* h, double* dt);
+ns2d_status ns2d_dt_range(const ns2d_handle* h, double* min_dt, double* max_dt);
+/* w_max_init of InitialConditions (solver.c:2003): reference value of the
+   vorticity-ratio step rule; captured on every ns2d_set_w_hat. */
+ns2d_status ns2d_set_w_max_init(ns2d_handle* h, double w_max_init);
+
+/* SystemCheck (solver.c:2301): NS2D_ERR_BLOWUP / _DT / _ITERS instead of exit(1). */
+ns2d_status ns2d_system_check(ns2d_handle* h, double dt, int64_t iters);
+
+/* ComputeSystemMeasurables (sys_msr.c:32).  spectra may be NULL; otherwise it
+   receives 8 * n_spect doubles: enrg, enst, d_enst_dt, enst_flux, enst_diss,
+   d_enrg_dt, enrg_flux, enrg_diss spectra.  With flux_diagnostics the RHS of
+   the state is evaluated first (with its conjugacy side effect, sys_msr.c:127). */
+ns2d_status ns2d_system_measurables(ns2d_handle* h, ns2d_measures* out, double* spectra);
+
+/* Real-space vorticity [nx][ny] (c2r of the state, normalised). */
+ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
+
+/* Execution control. */
+ns2d_status ns2d_set_stream(ns2d_handle* h, void* cuda_stream);
+ns2d_status ns2d_synchronize(ns2d_handle* h);
+/* Number of kernel launches issued by this handle since creation. */
+int64_t ns2d_launch_count(const ns2d_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
