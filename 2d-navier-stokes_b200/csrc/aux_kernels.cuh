@@ -1,0 +1,239 @@
+// aux_kernels.cuh -- transforms to real space with reductions (GetMaxData,
+// GetTimestep, real-space output) and small elementwise helpers.
+#pragma once
+#include "kernels.cuh"
+
+namespace ns2d {
+
+// Spectral source of one inverse x-FFT: element (i, j) at p[i*rs + j*es];
+// op 0 = as is, 1 = u_hat = ky (i/k^2) w, 2 = v_hat = -kx (i/k^2) w
+// (Solver/src/solver.c:2184-2196, 2393-2410).
+template <typename Real>
+struct InvField {
+    using C = typename Cx<Real>::T;
+    const C* p;
+    long long rs, es;
+    int op;
+    C* dst;  // [nx][ldc] x-space output
+};
+
+template <typename Real>
+struct InvArgs {
+    InvField<Real> f[2];
+    int nf;
+    int nyf, ldc;
+    const typename Cx<Real>::T* tw;
+    // op 1/2 wavenumbers for a scrambled index: kx from row i of the loop, the
+    // source element from the flat position (see cfl_scramble_kernel)
+};
+
+template <typename Real, int N, int TC>
+__global__ void __launch_bounds__(Plan<N>::T * TC) col_inv_kernel(InvArgs<Real> a) {
+    using C = typename Cx<Real>::T;
+    constexpr int T = Plan<N>::T;
+    constexpr int E = N / T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int c = threadIdx.x % TC;
+    const int t = threadIdx.x / TC;
+    const int ky = blockIdx.x * TC + c;
+    const bool valid = ky < a.nyf;
+    const int kyc = valid ? ky : 0;
+    for (int f = 0; f < a.nf; ++f) {
+        const InvField<Real> F = a.f[f];
+        C v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int i = t + T * m;
+            const int kx = (i <= N / 2) ? i : i - N;
+            C w = valid ? F.p[(long long)i * F.rs + (long long)kyc * F.es] : cmake<C>(0, 0);
+            if (F.op != 0) {
+                if (kx == 0 && ky == 0) {
+                    w = cmake<C>(0, 0);
+                } else {
+                    const double inv = 1.0 / (double)(kx * kx + ky * ky);
+                    if (F.op == 1) {
+                        const Real s = (Real)((double)ky * inv);
+                        w = cmake<C>(-s * w.y, s * w.x);
+                    } else {
+                        const Real s = (Real)((double)kx * inv);
+                        w = cmake<C>(s * w.y, -s * w.x);
+                    }
+                }
+            }
+            v[m] = w;
+        }
+        fft<N, +1, TC>(v, sm, a.tw, t, c);
+        if (valid) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) F.dst[(size_t)(t + T * m) * a.ldc + ky] = v[m];
+        }
+    }
+}
+
+enum RowC2ROp : int { R2_MAXABS = 0, R2_CFL = 1, R2_STORE = 2 };
+
+template <typename Real>
+struct RowC2RArgs {
+    using C = typename Cx<Real>::T;
+    const C* A;      // x-space field (real part of the output)
+    const C* B;      // x-space field (imaginary part), may be null
+    int ldc;
+    const C* tw;
+    double scale;    // 1/(Nx Ny)
+    double dx, dy;   // CFL
+    unsigned long long* maxbits;  // atomicMax target (bits of a non-negative double)
+    double* outA;    // R2_STORE: [nx][ny] real outputs
+    double* outB;
+};
+
+template <typename Real, int N, int PAIRS, int OP>
+__global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_c2r_kernel(RowC2RArgs<Real> a) {
+    using C = typename Cx<Real>::T;
+    constexpr int T = Plan<N>::T;
+    constexpr int E = N / T;
+    constexpr int TC = 2 * PAIRS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int g = threadIdx.x % TC;
+    const int t = threadIdx.x / TC;
+    const int x = blockIdx.x * TC + g;
+    const C* rA = a.A + (size_t)x * a.ldc;
+    const C* rB = a.B ? a.B + (size_t)x * a.ldc : nullptr;
+    C z[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int y = t + T * m;
+        const C zero = cmake<C>(0, 0);
+        if (y == 0 || y == N / 2) {
+            z[m] = cmake<C>(rA[y].x, rB ? rB[y].x : (Real)0);
+        } else if (y < N / 2) {
+            const C p = rA[y], q = rB ? rB[y] : zero;
+            z[m] = cmake<C>(p.x - q.y, p.y + q.x);
+        } else {
+            const C p = rA[N - y], q = rB ? rB[N - y] : zero;
+            z[m] = cmake<C>(p.x + q.y, q.x - p.y);
+        }
+    }
+    fft<N, +1, TC>(z, sm, a.tw, t, g);
+    double mx = 0.0;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int y = t + T * m;
+        const double u = (double)z[m].x * a.scale;
+        const double v = (double)z[m].y * a.scale;
+        if constexpr (OP == R2_MAXABS) {
+            mx = fmax(mx, fmax(fabs(u), fabs(v)));
+            if (!(u == u) || !(v == v)) mx = __longlong_as_double(0x7ff8000000000000ll);
+        } else if constexpr (OP == R2_CFL) {
+            // pi * (|u|/dx + |v|/dy)  (Solver/src/solver.c:2436-2438)
+            mx = fmax(3.14159265358979323846 * (fabs(u) / a.dx + fabs(v) / a.dy), mx);
+        } else {
+            a.outA[(size_t)x * N + y] = u;
+            if (a.outB) a.outB[(size_t)x * N + y] = v;
+        }
+    }
+    if constexpr (OP != R2_STORE) {
+        unsigned long long bits = (unsigned long long)__double_as_longlong(mx);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+            bits = other > bits ? other : bits;
+        }
+        if ((threadIdx.x & 31) == 0) atomicMax(a.maxbits, bits);
+    }
+}
+
+// CFL velocity spectrum with the reference's row index tmp = (i*Ny)/2 + 1
+// (Solver/src/solver.c:2393-2410), written into a persistent buffer with the
+// reference's interleaved [nx][nyf][2] layout; the state is read at the same
+// scrambled flat position.  Entries the loop never reaches keep their previous
+// contents, as in the reference.  Consecutive rows overlap by one element;
+// the reference's sequential loop leaves row i+1's j = 0 value there, so the
+// last element of every row but the last is not written here.
+template <typename Real>
+__global__ void cfl_scramble_kernel(const typename Cx<Real>::T* __restrict__ state, int ldc,
+                                    typename Cx<Real>::T* __restrict__ uhat, int nx, int ny, int quirk) {
+    using C = typename Cx<Real>::T;
+    const int nyf = ny / 2 + 1;
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf);
+        const int j = (int)(q % nyf);
+        if (quirk && j == nyf - 1 && i < nx - 1) continue;
+        const long long idx = quirk ? ((long long)i * ny / 2 + 1 + j) : q;
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        const int ky = j;
+        C u = cmake<C>(0, 0), v = cmake<C>(0, 0);
+        if (kx != 0 || ky != 0) {
+            const C w = state[(size_t)(idx / nyf) * ldc + (size_t)(idx % nyf)];
+            const double inv = 1.0 / (double)(kx * kx + ky * ky);
+            const Real su = (Real)((double)ky * inv);
+            const Real sv = (Real)((double)kx * inv);
+            u = cmake<C>(-su * w.y, su * w.x);
+            v = cmake<C>(sv * w.y, -sv * w.x);
+        }
+        uhat[2 * idx + 0] = u;
+        uhat[2 * idx + 1] = v;
+    }
+}
+
+// Pack/unpack between the reference layout [nx][nyf] (double) and the device
+// layout [nx][ldc] (Real).
+template <typename Real>
+__global__ void pack_kernel(const double2* __restrict__ src, typename Cx<Real>::T* __restrict__ dst, int nx, int nyf,
+                            int ldc) {
+    using C = typename Cx<Real>::T;
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), j = (int)(q % nyf);
+        const double2 s = src[q];
+        dst[(size_t)i * ldc + j] = cmake<C>((Real)s.x, (Real)s.y);
+    }
+}
+template <typename Real>
+__global__ void unpack_kernel(const typename Cx<Real>::T* __restrict__ src, double2* __restrict__ dst, int nx, int nyf,
+                              int ldc) {
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), j = (int)(q % nyf);
+        const auto s = src[(size_t)i * ldc + j];
+        dst[q] = make_double2((double)s.x, (double)s.y);
+    }
+}
+
+// ApplyDealiasing (Solver/src/solver.c:1039-1099) on `dim` interleaved fields
+// in the reference layout.
+template <typename Real>
+__global__ void dealias_kernel(typename Cx<Real>::T* a, int dim, int nx, int ny, int kmax_sqr, int dealias, int houli_int,
+                               int kolm) {
+    using C = typename Cx<Real>::T;
+    const int nyf = ny / 2 + 1;
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), ky = (int)(q % nyf);
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        const double k2 = (double)kx * kx + ky * ky;
+        for (int l = 0; l < dim; ++l) {
+            C v = a[q * dim + l];
+            if (dealias == 0) {
+                if (k2 >= (double)kmax_sqr || (kolm && kx == 0)) v = cmake<C>(0, 0);
+            } else {
+                v = cscale(v, houli_filter<Real>(kx, ky, nx, ny, houli_int));
+            }
+            a[q * dim + l] = v;
+        }
+    }
+}
+
+// ForceConjugacy (Solver/src/solver.c:2074-2107): state[kx<0, 0] = conj(src[|kx|, 0]).
+template <typename Real>
+__global__ void conj_kernel(typename Cx<Real>::T* state, int ldc, const typename Cx<Real>::T* src, long long src_stride,
+                            int nx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx || i <= nx / 2) return;
+    const int kx = i - nx;
+    state[(size_t)i * ldc] = cconj(src[(long long)(-kx) * src_stride]);
+}
+
+}  // namespace ns2d

@@ -1,0 +1,92 @@
+// engine.cuh -- per-grid-size launch tables for the step kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "aux_kernels.cuh"
+
+namespace ns2d {
+
+// Column-tile width (ky columns per block) and row pairs per block, chosen so
+// that blocks have about 128 threads.
+template <int N>
+struct Shape {
+    static constexpr int T = Plan<N>::T;
+    static constexpr int TC_RAW = 128 / T < 2 ? 2 : 128 / T;
+    static constexpr int TC = (N == 16) ? 8 : TC_RAW;
+    static constexpr int PAIRS_RAW = (128 / T) / 2 < 1 ? 1 : (128 / T) / 2;
+    static constexpr int PAIRS = PAIRS_RAW > N / 2 ? N / 2 : PAIRS_RAW;
+};
+
+template <typename Real, int N>
+struct Launch {
+    using C = typename Cx<Real>::T;
+    using S = Shape<N>;
+    static constexpr size_t col_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }
+    static constexpr size_t row_smem() {
+        size_t a = sizeof(C) * SmemLayout<N, 2 * S::PAIRS>::ELEMS;
+        size_t b = sizeof(Real) * N * 2 * S::PAIRS;
+        return a > b ? a : b;
+    }
+
+    static cudaError_t setup() {
+        cudaError_t e = cudaSuccess;
+        auto set = [&](const void* f, size_t bytes) {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        };
+        set((const void*)col_kernel<Real, N, S::TC, COL_P1>, col_smem());
+        set((const void*)col_kernel<Real, N, S::TC, COL_RHS>, col_smem());
+        set((const void*)col_kernel<Real, N, S::TC, COL_STAGE>, col_smem());
+        set((const void*)col_kernel<Real, N, S::TC, COL_FINAL>, col_smem());
+        set((const void*)row_kernel<Real, N, S::PAIRS>, row_smem());
+        set((const void*)col_inv_kernel<Real, N, S::TC>, col_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, row_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_CFL>, row_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_STORE>, row_smem());
+        return e;
+    }
+
+    static void col(int mode, const ColArgs<Real>& a, cudaStream_t s) {
+        dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
+        switch (mode) {
+            case COL_P1: col_kernel<Real, N, S::TC, COL_P1><<<grid, block, col_smem(), s>>>(a); break;
+            case COL_RHS: col_kernel<Real, N, S::TC, COL_RHS><<<grid, block, col_smem(), s>>>(a); break;
+            case COL_STAGE: col_kernel<Real, N, S::TC, COL_STAGE><<<grid, block, col_smem(), s>>>(a); break;
+            default: col_kernel<Real, N, S::TC, COL_FINAL><<<grid, block, col_smem(), s>>>(a); break;
+        }
+    }
+    static void row(const RowArgs<Real>& a, cudaStream_t s) {
+        dim3 grid(N / (2 * S::PAIRS)), block(S::T * 2 * S::PAIRS);
+        row_kernel<Real, N, S::PAIRS><<<grid, block, row_smem(), s>>>(a);
+    }
+    static void col_inv(const InvArgs<Real>& a, cudaStream_t s) {
+        dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
+        col_inv_kernel<Real, N, S::TC><<<grid, block, col_smem(), s>>>(a);
+    }
+    static void row_c2r(int op, const RowC2RArgs<Real>& a, cudaStream_t s) {
+        dim3 grid(N / (2 * S::PAIRS)), block(S::T * 2 * S::PAIRS);
+        switch (op) {
+            case R2_MAXABS: row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS><<<grid, block, row_smem(), s>>>(a); break;
+            case R2_CFL: row_c2r_kernel<Real, N, S::PAIRS, R2_CFL><<<grid, block, row_smem(), s>>>(a); break;
+            default: row_c2r_kernel<Real, N, S::PAIRS, R2_STORE><<<grid, block, row_smem(), s>>>(a); break;
+        }
+    }
+};
+
+// Runtime dispatch over the supported sizes.
+template <typename Real, typename F>
+inline bool with_size(int n, F&& f) {
+    switch (n) {
+        case 16: f(Launch<Real, 16>{}); return true;
+        case 32: f(Launch<Real, 32>{}); return true;
+        case 64: f(Launch<Real, 64>{}); return true;
+        case 128: f(Launch<Real, 128>{}); return true;
+        case 256: f(Launch<Real, 256>{}); return true;
+        case 512: f(Launch<Real, 512>{}); return true;
+        case 1024: f(Launch<Real, 1024>{}); return true;
+        case 2048: f(Launch<Real, 2048>{}); return true;
+        default: return false;
+    }
+}
+
+}  // namespace ns2d

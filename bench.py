@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""RK4 steps/s of the pseudospectral time step at 1024^2 (FP64), B200.
+
+Workload (the 1024^2 configuration of the headline metric): Kolmogorov-forced
+flow, n = 4, F = 1, nu = 1e-4 plus hyperviscosity nu_h |k|^16 (nu_h = 2e-40)
+through the RK4CN drag branch, dt = 2.5e-4, 2/3 dealiasing, FP64, from seeded
+1e-3-amplitude random-phase noise (synthetic input; no dataset involved).
+
+One "step" = one RK4CN step (4 nonlinear-term evaluations + update) of one
+1024^2 trajectory.  With --gpus N (torchrun, one process per GPU) every rank
+advances its own trajectory (replicas: the path has no exchange step), so
+`value` is the job's total steps/s and scaling is weak.
+
+  value   device time (CUDA events on the solver's stream) per step, state
+          resident in HBM; L2 is flushed (256 MiB write) between timed steps,
+          outside the events.
+  e2e     ns2d_rk4_step_host: the reference-facing RK4Step contract with the
+          state in pinned host memory, copied in and out every step (wall
+          clock per step, L2 flushed between steps).
+  --impl reference   the reference's own CPU solver (Solver/src built by
+          oracle/Makefile; FFTW replaced by the oracle's FFT) on the host cores.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "2d-navier-stokes_b200"), os.path.join(ROOT, "oracle")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "RK4 steps/s at 1024^2 (FP64 plain vs FP32 batched); adjoint/forward time"
+N = 1024
+DT = 2.5e-4
+NU_H = 2e-40
+WORKLOAD = "kolmogorov_1024_fp64_rk4cn"
+S_BYTES = 16 * N * (N // 2 + 1)  # one FP64 half spectrum
+# algorithmic bytes per launch, in units of S, per kernel class:
+# 0 column pass P1 (read 1, write 4), 1 column pass with stage combine (read
+# n, w, acc; write acc + 4 fields: 8; stage 1 has no acc read: 7), 2 final
+# column pass (read n, w, acc; write w: 4), 3 row pass (read 4, write 1).
+CLASS_NAMES = ["col_p1", "col_stage", "col_final", "row", "other"]
+CLASS_BYTES_PER_STEP = {0: 5, 1: 7 + 8 + 8, 2: 4, 3: 4 * 5}
+MODEL_BYTES_PER_STEP = 58  # the 2-pass minimal model (58 S per RK4 step)
+
+
+def params(device=0):
+    from ns2d import abi
+    return abi.default_params(nx=N, ny=N, nu=1e-4, ekmn_drag_flag=1, ekmn_alpha=NU_H, ekmn_drag_pow=8.0,
+                              forcing=abi.FORCING_KOLM, force_k=4, force_scale=1.0, dt=DT, device=device)
+
+
+def config(parallelism):
+    return {"workload": WORKLOAD, "grid": f"{N}x{N}", "nu": 1e-4, "nu_h": NU_H, "hyperviscosity": "|k|^16",
+            "dt": DT, "forcing": "KOLM n=4 F=1", "integrator": "RK4CN", "dealias": "2/3",
+            "l2": "flushed between timed steps (256 MiB write outside the timed events)",
+            "parallelism": parallelism}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(cls):
+    """DRAM bytes per launch for a kernel class from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "col_row_1024_fp64.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"traffic_bytes_per_launch\s+{CLASS_NAMES[cls]}\s+([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(steps, warmup, threads, budget_s=None):
+    """The reference's own solver (oracle/_ref) on the host: steps/s."""
+    from ns2d import initial
+    from pyoracle import RefSolver, build, ref_available
+    if not ref_available("rk4cn"):
+        build(ref=True)
+    ref = RefSolver(params(), "rk4cn", threads=threads)
+    ref.set_w_hat(initial.noise(N, seed=7, amplitude=1e-3, kolm=True))
+    for _ in range(warmup):
+        ref.rk4_step(DT)
+    if budget_s is not None:
+        t0 = time.perf_counter()
+        ref.rk4_step(DT)
+        one = time.perf_counter() - t0
+        steps = max(2, min(steps, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.rk4_step(DT)
+    el = time.perf_counter() - t0
+    return steps / el, steps, el
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    value, steps, el = cpu_reference(args.steps, args.warmup, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config("reference CPU (1 process, OpenMP FFT)"),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "reference",
+                             "sample": f"{steps} RK4CN steps of the {N}^2 Kolmogorov workload: the reference's "
+                                       "Solver/src (solver.c, force.c, sys_msr.c) built by oracle/Makefile, "
+                                       "FFTW-MPI replaced by the oracle's OpenMP FFT"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from ns2d import Solver, initial
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    s = Solver(params(local_rank))
+    stream = torch.cuda.Stream(device=dev)
+    s.set_stream(stream.cuda_stream)
+    w0 = initial.noise(N, seed=7 + rank, amplitude=1e-3, kolm=True)
+    s.set_w_hat(w0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    s.step_async(args.warmup, DT)
+    s.check()
+    # timed region: K steps, each bracketed by events; L2 flush between them
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    s.set_kernel_timing(True)
+    l0 = s.launch_count
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for e0, e1 in evs:
+                e0.record(stream)
+                s.step_async(1, DT)
+                e1.record(stream)
+                flush.zero_()
+        torch.cuda.synchronize(dev)
+        s.check()
+    launches = s.launch_count - l0
+    barrier()
+    ms_total = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    kms, kn = s.kernel_times()
+    s.set_kernel_timing(False)
+    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max * 1e-3)
+
+    # end to end through the reference-facing host-buffer call
+    host = torch.empty((N, N // 2 + 1, 2), dtype=torch.float64, pin_memory=True)
+    hw = host.numpy().view(np.complex128).reshape(N, N // 2 + 1)
+    hw[:] = w0
+    ke = max(3, min(args.steps, 20))
+    s.rk4_step_host(hw, DT)
+    walls = []
+    barrier()
+    for _ in range(ke):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.rk4_step_host(hw, DT)
+        walls.append(time.perf_counter() - t0)
+    te = torch.tensor([sum(walls)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * ke / float(te.item())
+
+    if rank != 0:
+        s.close()
+        return 0
+
+    # roofline of the dominant kernel class
+    peak, peak_kind = peaks()
+    dom = int(np.argmax(kms[:4]))
+    per_launch_bytes = CLASS_BYTES_PER_STEP[dom] * S_BYTES / (kn[dom] / args.steps)
+    avg_ms = kms[dom] / kn[dom]
+    achieved = per_launch_bytes / (avg_ms * 1e-3) / 1e9
+    step_ms = ms_max / args.steps
+    model_gbs = MODEL_BYTES_PER_STEP * S_BYTES / (step_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-phase noise, 1e-3 amplitude)",
+        "config": config("replicas" if world > 1 else "single GPU"),
+        "roofline": {"bound": "hbm", "kernel": CLASS_NAMES[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": ncu_traffic(dom), "algorithmic_bytes_per_launch": per_launch_bytes},
+        "step_roofline": {"model_bytes_per_step": MODEL_BYTES_PER_STEP * S_BYTES, "achieved": model_gbs,
+                          "frac": model_gbs / peak, "unit": "GB/s"},
+        "kernels": {CLASS_NAMES[k]: {"ms_total": float(kms[k]), "launches": int(kn[k]),
+                                     "share": float(kms[k] / max(kms.sum(), 1e-30))} for k in range(5) if kn[k]},
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": S_BYTES, "d2h_bytes_per_step": S_BYTES,
+                "call": "ns2d_rk4_step_host"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, st, el = cpu_reference(1000, 1, threads, budget_s=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
+                                "sample": f"{st} RK4CN steps ({el:.1f} s) of the same {N}^2 workload on the host: "
+                                          "the reference's Solver/src built by oracle/Makefile, FFTW-MPI replaced "
+                                          "by the oracle's OpenMP FFT"}
+    print(json.dumps(line), flush=True)
+    s.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ns2d", choices=["ns2d", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

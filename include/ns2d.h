@@ -154,6 +154,18 @@ ns2d_status ns2d_ab4_step(ns2d_handle* h, double dt, int32_t iters);
    (the loop body of SpectralSolve, solver.c:142-236, minus saving). */
 ns2d_status ns2d_step_n(ns2d_handle* h, int32_t nsteps, double dt);
 
+/* RK4Step with the state in host memory, as the reference keeps it in
+   run_data->w_hat (solver.c:625): copies w_hat in, steps, copies it back.
+   The drop-in form for callers that own a host array. */
+ns2d_status ns2d_rk4_step_host(ns2d_handle* h, double* w_hat, double dt);
+
+/* Enqueue nsteps fixed-dt steps on the handle's stream and return without
+   waiting.  Failures detected on the device (SystemCheck) are reported by the
+   next ns2d_check. */
+ns2d_status ns2d_step_async(ns2d_handle* h, int32_t nsteps, double dt);
+/* Wait for queued work and apply SystemCheck (solver.c:2301) to it. */
+ns2d_status ns2d_check(ns2d_handle* h);
+
 /* ApplyDealiasing (solver.c:1039) on a host array of array_dim interleaved
    spectral fields, in place. */
 ns2d_status ns2d_apply_dealiasing(ns2d_handle* h, double* arr, int32_t array_dim);
@@ -187,6 +199,14 @@ ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
 
 /* Execution control. */
 ns2d_status ns2d_set_stream(ns2d_handle* h, void* cuda_stream);
+ns2d_status ns2d_get_stream(const ns2d_handle* h, void** cuda_stream);
+/* Per-kernel timing with CUDA events on the handle's stream.  Kernel classes:
+   0 column pass (inverse transforms only), 1 column pass with RK stage
+   combine, 2 column pass with the final update, 3 row pass, 4 other. */
+#define NS2D_KERNEL_CLASSES 5
+ns2d_status ns2d_set_kernel_timing(ns2d_handle* h, int32_t enable);
+/* Totals since timing was enabled (waits for the stream). */
+ns2d_status ns2d_kernel_times(ns2d_handle* h, double* ms_total, int64_t* launches, int32_t nclasses);
 ns2d_status ns2d_synchronize(ns2d_handle* h);
 /* Number of kernel launches issued by this handle since creation. */
 int64_t ns2d_launch_count(const ns2d_handle* h);

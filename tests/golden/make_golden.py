@@ -1,0 +1,130 @@
+"""Generate tests/golden/*.npz from the reference solver's own sources.
+
+Runs oracle/_ref/libns2d_ref_<variant>.so (Solver/src/{solver,force,sys_msr}.c
+compiled unmodified by oracle/Makefile against single-rank MPI/FFTW stand-ins)
+on small seeded cases and stores inputs, parameters and outputs.  Each case
+runs in a fresh process because the reference keeps its state in globals.
+
+    python tests/golden/make_golden.py          # needs the reference sources
+"""
+import multiprocessing as mp
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "2d-navier-stokes_b200"), os.path.join(ROOT, "oracle")]
+
+from ns2d import abi, initial  # noqa: E402
+
+
+def cases():
+    """name -> (variant, params kwargs, initial condition spec, program)."""
+    return {
+        # BASELINE config 1 shape: Taylor-Green, nu|k|^2 via the drag-flag recipe
+        # of InitFiles/TaylorGreen/tg.ini (EKMN_DRAG_FLAG = 1, alpha = 0).
+        "tg64_rk4cn": ("rk4cn", dict(nx=64, ny=64, nu=0.01, ekmn_drag_flag=1, ekmn_alpha=0.0, dt=1e-3),
+                       ("tg",), [("steps", 100, 1e-3), ("w_hat",), ("max", 0), ("meas",)]),
+        # stock flags: hyperviscosity latch (nu |k|^4), decaying spectrum
+        "dec64_rk4cn": ("rk4cn", dict(nx=64, ny=64, nu=1e-3, dt=1e-3),
+                        ("decaying", 11, 6.0), [("rhs_state",), ("steps", 20, 1e-3), ("w_hat",), ("meas",),
+                                                ("max", 0), ("max", 1), ("cfl", 1e-3), ("w_hat",)]),
+        # Kolmogorov forcing n = 4, F = 1, nu k^2 + hyperviscosity alpha k^16
+        "kolm64_rk4cn": ("rk4cn", dict(nx=64, ny=64, nu=1e-3, ekmn_drag_flag=1, ekmn_alpha=1e-20,
+                                        ekmn_drag_pow=8.0, forcing=abi.FORCING_KOLM, force_k=4, force_scale=1.0,
+                                        dt=2.5e-3),
+                         ("noise", 5), [("steps", 30, 2.5e-3), ("w_hat",), ("meas",), ("max", 0)]),
+        # explicit RK4 with the reference's +D X stage term
+        "dec32_rk4": ("rk4", dict(nx=32, ny=32, nu=1e-3, integrator=abi.RK4, ekmn_drag_flag=1, dt=1e-3),
+                      ("decaying", 3, 4.0), [("steps", 10, 1e-3), ("w_hat",)]),
+        # AB4 with three RK4CN start-up steps
+        "dec32_ab4": ("ab4", dict(nx=32, ny=32, nu=1e-3, integrator=abi.AB4, dt=1e-3),
+                      ("decaying", 4, 4.0), [("ab4", 10, 1e-3), ("w_hat",)]),
+        # one RHS of an input whose ky = 0 column is not Hermitian (FFTW c2r
+        # reads only the real parts there) and the conjugacy side effect
+        "nonherm32_rhs": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, dt=1e-3),
+                          ("decaying", 5, 4.0), [("rhs_input", 77), ("w_hat",)]),
+        # adaptive CFL step with the reference's row-index quirk
+        "cfl32": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9, dt=1e-3),
+                  ("decaying", 6, 4.0), [("cfl", 1e-3), ("steps", 5, 2e-3), ("cfl", 2e-3), ("w_hat",)]),
+    }
+
+
+def make_ic(spec, n):
+    if spec[0] == "tg":
+        return initial.taylor_green(n)
+    if spec[0] == "decaying":
+        return initial.decaying(n, seed=spec[1], k0=spec[2], dealias="2/3")
+    if spec[0] == "noise":
+        return initial.noise(n, seed=spec[1], amplitude=1e-3, kolm=True)
+    raise ValueError(spec)
+
+
+def run_program(solver, w0, program, record):
+    solver.set_w_hat(w0)
+    outs = []
+    for op in program:
+        kind = op[0]
+        if kind == "steps":
+            for _ in range(op[1]):
+                solver.rk4_step(op[2])
+        elif kind == "ab4":
+            for it in range(1, op[1] + 1):
+                solver.ab4_step(op[2], it)
+        elif kind == "w_hat":
+            outs.append(solver.get_w_hat())
+        elif kind == "max":
+            outs.append(np.array([solver.get_max_data(op[1])]))
+        elif kind == "cfl":
+            outs.append(np.array([solver.get_timestep(op[1])]))
+        elif kind == "meas":
+            s, sp = solver.system_measurables()
+            outs.append(np.asarray(s))
+            outs.append(np.asarray(sp))
+        elif kind == "rhs_state":
+            outs.append(solver.nonlinear_rhs(None))
+        elif kind == "rhs_input":
+            rng = np.random.default_rng(op[1])
+            x = w0 + 1e-3 * np.abs(w0).max() * (rng.standard_normal(w0.shape) + 1j * rng.standard_normal(w0.shape))
+            x[:, 0] += 0.01 * np.abs(w0).max() * rng.standard_normal(w0.shape[0])  # non-Hermitian column 0
+            outs.append(x)
+            outs.append(solver.nonlinear_rhs(x))
+        else:
+            raise ValueError(kind)
+    return outs
+
+
+def _ref_worker(name, q):
+    from pyoracle import RefSolver
+    variant, kw, ic, program = cases()[name]
+    p = abi.default_params(**kw)
+    w0 = make_ic(ic, p.nx)
+    ref = RefSolver(p, variant)
+    q.put(run_program(ref, w0, program, True))
+
+
+def generate(name):
+    variant, kw, ic, program = cases()[name]
+    p = abi.default_params(**kw)
+    w0 = make_ic(ic, p.nx)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    proc = ctx.Process(target=_ref_worker, args=(name, q))
+    proc.start()
+    outs = q.get(timeout=600)
+    proc.join()
+    params = {f: getattr(p, f) for f, _ in abi.Params._fields_}
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), w0=w0, n_out=len(outs),
+                        params=np.array([float(params[f]) for f, _ in abi.Params._fields_]),
+                        param_names=np.array([f for f, _ in abi.Params._fields_]),
+                        variant=variant, **{f"out{i}": o for i, o in enumerate(outs)})
+    return len(outs)
+
+
+if __name__ == "__main__":
+    import pyoracle
+    pyoracle.build(ref=True)
+    for name in cases():
+        print(name, generate(name))

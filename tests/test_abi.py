@@ -1,0 +1,80 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol that
+include/ns2d.h declares, and agrees with the ctypes mirror."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from ns2d import abi
+from ns2d._lib import LIB_PATH, exported_symbols, load
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_header_symbols():
+    assert os.path.exists(LIB_PATH), "libns2d.so not built"
+    names = exported_symbols()
+    assert len(names) >= 25
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], capture_output=True, text=True, check=True).stdout
+    defined = set(re.findall(r"\sT\s(\w+)", out))
+    missing = [n for n in names if n not in defined]
+    assert not missing, missing
+
+
+def test_library_loads_and_defaults_match_reference_cli():
+    L = load()
+    p = abi.Params()
+    assert L.ns2d_params_default(C.byref(p)) == abi.OK
+    q = abi.default_params()
+    for name, _ in abi.Params._fields_:
+        assert getattr(p, name) == getattr(q, name), name
+    # Solver/src/utils.c:57-83
+    assert (p.nx, p.ny, p.nu, p.dt, p.cfl_const) == (64, 64, 1e-4, 1e-4, 0.9)
+    assert L.ns2d_status_string(abi.ERR_BLOWUP) == b"NS2D_ERR_BLOWUP"
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """Compile a probe against include/ns2d.h and compare every field offset."""
+    fields = [n for n, _ in abi.Params._fields_]
+    mfields = [n for n, _ in abi.Measures._fields_]
+    body = "\n".join(f'printf("P {n} %zu\\n", offsetof(ns2d_params, {n}));' for n in fields)
+    body += "\n" + "\n".join(f'printf("M {n} %zu\\n", offsetof(ns2d_measures, {n}));' for n in mfields)
+    prog = tmp_path / "probe.c"
+    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ns2d.h"\nint main(void){\n'
+                    + body + '\nprintf("S %zu %zu\\n", sizeof(ns2d_params), sizeof(ns2d_measures));return 0;}\n')
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    for line in out:
+        parts = line.split()
+        if not parts:
+            continue
+        if parts[0] == "P":
+            assert getattr(abi.Params, parts[1]).offset == int(parts[2]), parts[1]
+        elif parts[0] == "M":
+            assert getattr(abi.Measures, parts[1]).offset == int(parts[2]), parts[1]
+        else:
+            assert (C.sizeof(abi.Params), C.sizeof(abi.Measures)) == (int(parts[1]), int(parts[2]))
+
+
+def test_create_without_device_reports_no_device():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("device present")
+    except Exception:
+        pass
+    L = load()
+    p = abi.default_params()
+    h = C.c_void_p()
+    assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_NO_DEVICE
+
+
+def test_invalid_sizes_rejected_before_device_use():
+    L = load()
+    for nx, ny in ((96, 96), (64, 32), (8, 8), (4096, 4096)):
+        p = abi.default_params(nx=nx, ny=ny)
+        h = C.c_void_p()
+        assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED

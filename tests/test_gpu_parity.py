@@ -1,0 +1,206 @@
+"""GPU parity: libns2d.so (through its C ABI) against the reference's golden
+outputs and against the oracle restatement.
+
+Tolerances (FP64): single RHS evaluation 1e-13 of max|RHS|; w_hat after up to
+100 RK4CN steps 1e-12 of max|w_hat| (the target stated for the plain form);
+measurable totals 1e-11 relative; maxima and CFL step 1e-12 relative.
+FP32 form: 5e-5 of max for one RHS, 1e-4 for the state after 100 steps.
+"""
+import numpy as np
+import pytest
+
+from _util import load_case, make_golden, rel_err
+from ns2d import Solver, abi, initial
+from pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+CASES = sorted(make_golden.cases())
+
+
+def _tol(kind):
+    return {"w_hat": 1e-12, "rhs": 1e-13, "meas": 1e-11, "spec": 1e-11, "scalar": 1e-12}[kind]
+
+
+def _kinds(program):
+    kinds = []
+    for op in program:
+        if op[0] in ("w_hat",):
+            kinds.append("w_hat")
+        elif op[0] in ("max", "cfl"):
+            kinds.append("scalar")
+        elif op[0] == "meas":
+            kinds += ["meas", "spec"]
+        elif op[0] == "rhs_state":
+            kinds.append("rhs")
+        elif op[0] == "rhs_input":
+            kinds += ["input", "rhs"]
+    return kinds
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_matches_reference_fixture(name):
+    p, w0, ref_outs = load_case(name)
+    _, _, _, program = make_golden.cases()[name]
+    s = Solver(p)
+    outs = make_golden.run_program(s, w0, program, False)
+    for k, (a, b, kind) in enumerate(zip(outs, ref_outs, _kinds(program))):
+        if kind == "input":
+            continue
+        if kind == "meas":
+            # divergence (index 4) is rounding noise around 0: compare absolutely
+            for q in range(len(b)):
+                if q == 4:
+                    assert abs(a[q]) < 1e-20 + 1e-12 * abs(b[1]), (name, k, q, a[q], b[q])
+                else:
+                    assert abs(a[q] - b[q]) <= _tol("meas") * max(abs(b[q]), 1e-300), (name, k, q, a[q], b[q])
+            continue
+        assert rel_err(a, b) <= _tol(kind), (name, k, kind, rel_err(a, b))
+    s.close()
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048])
+def test_rhs_every_grid_size(n):
+    p = abi.default_params(nx=n, ny=n, nu=1e-3)
+    w0 = initial.decaying(n, seed=100 + n, k0=min(6.0, n / 8), dealias="2/3")
+    o = Oracle(p, threads=8)
+    o.set_w_hat(w0)
+    ref = o.nonlinear_rhs(None)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    got = s.nonlinear_rhs(None)
+    assert rel_err(got, ref) <= 1e-13, (n, rel_err(got, ref))
+    # conjugacy side effect on the state
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-15
+    s.close()
+
+
+def test_kolmogorov_1024_fp64_steps():
+    """BASELINE config 3 (FP64): Kolmogorov n = 4, F = 1, nu = 1e-4 plus
+    hyperviscosity nu_h k^16 through the RK4CN drag branch, dt = 2.5e-4."""
+    n = 1024
+    p = abi.default_params(nx=n, ny=n, nu=1e-4, ekmn_drag_flag=1, ekmn_alpha=2e-40, ekmn_drag_pow=8.0,
+                           forcing=abi.FORCING_KOLM, force_k=4, force_scale=1.0, dt=2.5e-4)
+    w0 = initial.noise(n, seed=7, amplitude=1e-3, kolm=True)
+    o = Oracle(p, threads=8)
+    o.set_w_hat(w0)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    for _ in range(5):
+        o.rk4_step(2.5e-4)
+        s.rk4_step(2.5e-4)
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-12
+    m_gpu, sp_gpu = s.system_measurables()
+    m_ref, sp_ref = o.system_measurables()
+    for q in (0, 1, 2, 3, 5, 6):
+        assert abs(m_gpu[q] - m_ref[q]) <= 1e-11 * abs(m_ref[q]), q
+    s.close()
+
+
+def test_decaying_256_houli_cfl():
+    """BASELINE config 2 shape: 256^2, nu = 5e-4, Hou-Li filter (reference's
+    integer form), CFL 0.9 adaptive step; 20 steps with dt from GetTimestep."""
+    n = 256
+    p = abi.default_params(nx=n, ny=n, nu=5e-4, dealias=abi.DEALIAS_HOU_LI, adapt_step_flag=1,
+                           cfl_cond_flag=1, cfl_const=0.9, dt=1e-3)
+    w0 = initial.decaying(n, seed=2, k0=6.0)
+    o = Oracle(p, threads=8)
+    o.set_w_hat(w0)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    dt_o = o.get_timestep(p.dt)
+    dt_s = s.get_timestep(p.dt)
+    for _ in range(20):
+        assert abs(dt_s - dt_o) <= 1e-12 * dt_o
+        o.rk4_step(dt_o)
+        s.rk4_step(dt_s)
+        dt_o = o.get_timestep(dt_o)
+        dt_s = s.get_timestep(dt_s)
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-12
+    s.close()
+
+
+def test_step_n_equals_repeated_steps():
+    n = 128
+    p = abi.default_params(nx=n, ny=n, nu=1e-3, dt=1e-3)
+    w0 = initial.decaying(n, seed=9, k0=6.0, dealias="2/3")
+    a = Solver(p)
+    b = Solver(p)
+    a.set_w_hat(w0)
+    b.set_w_hat(w0)
+    for _ in range(7):
+        a.rk4_step(1e-3)
+    b.step_n(7, 1e-3)
+    assert np.array_equal(a.get_w_hat(), b.get_w_hat())
+    a.close()
+    b.close()
+
+
+def test_ab4_step_n_matches_oracle():
+    n = 64
+    p = abi.default_params(nx=n, ny=n, nu=1e-3, integrator=abi.AB4, dt=1e-3)
+    w0 = initial.decaying(n, seed=12, k0=5.0, dealias="2/3")
+    o = Oracle(p)
+    o.set_w_hat(w0)
+    for it in range(1, 21):
+        o.ab4_step(1e-3, it)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    s.step_n(20, 1e-3)
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-12
+    s.close()
+
+
+def test_real_space_vorticity_and_max():
+    n = 128
+    p = abi.default_params(nx=n, ny=n, nu=1e-3)
+    w0 = initial.decaying(n, seed=4, k0=6.0, dealias="2/3")
+    o = Oracle(p)
+    o.set_w_hat(w0)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    assert rel_err(s.get_w_real(), o.get_w_real()) <= 1e-13
+    assert abs(s.get_max_data(abi.MAX_VORT) - o.get_max_data(abi.MAX_VORT)) <= 1e-13 * o.get_max_data(0)
+    assert abs(s.get_max_data(abi.MAX_VEL) - o.get_max_data(abi.MAX_VEL)) <= 1e-13 * o.get_max_data(1)
+    s.close()
+
+
+def test_blowup_reported_not_exit():
+    """SystemCheck exits the process in the reference (solver.c:2314); here a
+    non-finite state makes step_n return NS2D_ERR_BLOWUP."""
+    from ns2d import NS2DError
+    n = 64
+    p = abi.default_params(nx=n, ny=n, nu=1e-3)
+    w0 = initial.decaying(n, seed=1, k0=5.0, dealias="2/3")
+    w0[3, 2] = np.nan
+    s = Solver(p)
+    s.set_w_hat(w0)
+    with pytest.raises(NS2DError) as e:
+        s.step_n(5, 1e-3)
+    assert e.value.status == abi.ERR_BLOWUP
+    # the handle stays usable
+    s.set_w_hat(initial.decaying(n, seed=1, k0=5.0, dealias="2/3"))
+    s.step_n(2, 1e-3)
+    assert np.isfinite(s.get_w_hat()).all()
+    s.close()
+
+
+def test_fp32_form_error_vs_fp64():
+    n = 128
+    p64 = abi.default_params(nx=n, ny=n, nu=1e-3)
+    p32 = abi.default_params(nx=n, ny=n, nu=1e-3, precision=abi.FP32)
+    w0 = initial.decaying(n, seed=21, k0=6.0, dealias="2/3")
+    o = Oracle(p64)
+    o.set_w_hat(w0)
+    ref = o.nonlinear_rhs(None)
+    s = Solver(p32)
+    s.set_w_hat(w0)
+    assert rel_err(s.nonlinear_rhs(None), ref) <= 5e-5
+    for _ in range(100):
+        o.rk4_step(1e-3)
+    s.step_n(100, 1e-3)
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-4
+    z_ref = initial.enstrophy(o.get_w_hat())
+    z_32 = initial.enstrophy(s.get_w_hat())
+    assert abs(z_32 - z_ref) <= 1e-5 * z_ref
+    s.close()
