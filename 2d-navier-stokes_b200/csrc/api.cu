@@ -286,14 +286,15 @@ ns2d_status ab4_update_impl(ns2d_handle* h, double dt) {
     ColArgs<Real> a;
     fill_common<Real>(h, a, branch);
     a.src = (const C*)h->state;
+    a.col0_out = (C*)h->col0[0];  // the final pass rewrites the state's column 0
     launch_col<Real>(h, COL_P1, a);
     launch_row<Real>(h);
     fill_common<Real>(h, a, branch);
     a.src = (const C*)h->nl;
     a.dt = dt;
     a.conj_mode = 1;
-    a.conj_src = (const C*)h->state;
-    a.conj_stride = h->ldc;
+    a.conj_src = (const C*)h->col0[0];
+    a.conj_stride = 1;
     a.scheme = euler ? 3 : 2;
     a.h0 = (const C*)h->ab[0];
     a.h1 = (const C*)h->ab[1];
@@ -440,7 +441,8 @@ template <typename Real>
 ns2d_status create_impl(ns2d_handle* h) {
     using C = Cplx<Real>;
     const size_t fb = h->field_bytes;
-    void** fields[] = {&h->state, &h->acc, &h->nl, &h->f[0], &h->f[1], &h->f[2], &h->f[3], &h->tmpfull, &h->rhsbuf};
+    void** fields[] = {&h->state, &h->acc,   &h->nl,    &h->f[0],  &h->f[1],  &h->f[2], &h->f[3],
+                       &h->tmpfull, &h->rhsbuf, &h->ab[0], &h->ab[1], &h->ab[2], &h->ab[3]};
     for (void** p : fields) {
         CK(h, cudaMalloc(p, fb));
         CK(h, cudaMemsetAsync(*p, 0, fb, h->stream));

@@ -21,8 +21,10 @@ template <typename Real, int N>
 struct Launch {
     using C = typename Cx<Real>::T;
     using S = Shape<N>;
-    static constexpr size_t col_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }
-    static constexpr size_t row_smem() {
+    static constexpr size_t col_smem() { return ColSmem<Real, N, S::TC>::bytes(); }
+    static constexpr size_t row_smem() { return RowSmem<Real, N, 2 * S::PAIRS>::bytes(); }
+    static constexpr size_t inv_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }
+    static constexpr size_t c2r_smem() {
         size_t a = sizeof(C) * SmemLayout<N, 2 * S::PAIRS>::ELEMS;
         size_t b = sizeof(Real) * N * 2 * S::PAIRS;
         return a > b ? a : b;
@@ -39,10 +41,10 @@ struct Launch {
         set((const void*)col_kernel<Real, N, S::TC, COL_STAGE>, col_smem());
         set((const void*)col_kernel<Real, N, S::TC, COL_FINAL>, col_smem());
         set((const void*)row_kernel<Real, N, S::PAIRS>, row_smem());
-        set((const void*)col_inv_kernel<Real, N, S::TC>, col_smem());
-        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, row_smem());
-        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_CFL>, row_smem());
-        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_STORE>, row_smem());
+        set((const void*)col_inv_kernel<Real, N, S::TC>, inv_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, c2r_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_CFL>, c2r_smem());
+        set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_STORE>, c2r_smem());
         return e;
     }
 
@@ -61,14 +63,14 @@ struct Launch {
     }
     static void col_inv(const InvArgs<Real>& a, cudaStream_t s) {
         dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
-        col_inv_kernel<Real, N, S::TC><<<grid, block, col_smem(), s>>>(a);
+        col_inv_kernel<Real, N, S::TC><<<grid, block, inv_smem(), s>>>(a);
     }
     static void row_c2r(int op, const RowC2RArgs<Real>& a, cudaStream_t s) {
         dim3 grid(N / (2 * S::PAIRS)), block(S::T * 2 * S::PAIRS);
         switch (op) {
-            case R2_MAXABS: row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS><<<grid, block, row_smem(), s>>>(a); break;
-            case R2_CFL: row_c2r_kernel<Real, N, S::PAIRS, R2_CFL><<<grid, block, row_smem(), s>>>(a); break;
-            default: row_c2r_kernel<Real, N, S::PAIRS, R2_STORE><<<grid, block, row_smem(), s>>>(a); break;
+            case R2_MAXABS: row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS><<<grid, block, c2r_smem(), s>>>(a); break;
+            case R2_CFL: row_c2r_kernel<Real, N, S::PAIRS, R2_CFL><<<grid, block, c2r_smem(), s>>>(a); break;
+            default: row_c2r_kernel<Real, N, S::PAIRS, R2_STORE><<<grid, block, c2r_smem(), s>>>(a); break;
         }
     }
 };

@@ -34,6 +34,10 @@ struct LinOp {
     int hp_int, dp_int;  // exponents when integral, else INT_MIN
 };
 
+// Out of line: the callers sit in fully unrolled per-element loops, and one
+// shared copy of this code keeps the kernels inside the instruction cache.
+__device__ __noinline__ double pow_general(double x, double p) { return pow(x, p); }
+
 __device__ __forceinline__ double powk(double k2, double p, int pint) {
     if (pint != -2147483647 - 1) {
         int e = pint < 0 ? -pint : pint;
@@ -45,7 +49,7 @@ __device__ __forceinline__ double powk(double k2, double p, int pint) {
         }
         return pint < 0 ? 1.0 / r : r;
     }
-    return pow(k2, p);
+    return pow_general(k2, p);
 }
 
 __device__ __forceinline__ double lin_bracket(const LinOp& L, double k2) {
@@ -113,7 +117,7 @@ __device__ __forceinline__ bool block_should_exit(const int* status) {
 }
 
 template <typename Real>
-__device__ __forceinline__ Real houli_filter(int kx, int ky, int nx, int ny, int quirk) {
+__device__ __noinline__ Real houli_filter(int kx, int ky, int nx, int ny, int quirk) {
     double fx, fy;
     if (quirk) {
         fx = (double)(kx / (nx / 2));
@@ -133,39 +137,109 @@ __device__ __forceinline__ Real houli_filter(int kx, int ky, int nx, int ny, int
     return (Real)exp(-e);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80+ PTX).
+template <typename C>
+__device__ __forceinline__ void cp_async_elem(C* smem, const C* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(C) == 16) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared memory of the column pass: the FFT exchange buffer, then two
+// [N][TC] staging arrays (state or stage input, and the RK accumulator).
+template <typename Real, int N, int TC>
+struct ColSmem {
+    using C = typename Cx<Real>::T;
+    static constexpr int FFT = SmemLayout<N, TC>::ELEMS;
+    static constexpr int PRE = N * TC;
+    static constexpr size_t bytes() { return sizeof(C) * (size_t)(FFT + 2 * PRE); }
+};
+
+// Derived spectrum f of the stage input X at (kx, ky) (solver.c:904-957):
+// 0: i ky/k^2 X, 1: -i kx/k^2 X, 2: i kx X, 3: i ky X.
+template <typename C>
+__device__ __forceinline__ C derived(int f, int kx, int ky, C X) {
+    using Real = decltype(C::x);
+    if (kx == 0 && ky == 0) return cmake<C>(0, 0);
+    Real s;
+    if (f < 2) {
+        const double inv = 1.0 / (double)(kx * kx + ky * ky);
+        s = (Real)((double)(f == 0 ? ky : kx) * inv);
+    } else {
+        s = (Real)(f == 2 ? kx : ky);
+    }
+    return (f == 1) ? cmake<C>(s * X.y, -s * X.x) : cmake<C>(-s * X.y, s * X.x);
+}
+
 // Column pass.  Grid: ceil(nyf / TC) blocks; block: T * TC threads, thread
-// (t, c) with c = threadIdx.x % TC.  Dynamic shared memory: SmemLayout ELEMS.
+// (t, c) with c = threadIdx.x % TC.  Dynamic shared memory: ColSmem::bytes().
 template <typename Real, int N, int TC, int MODE>
 __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
+    using SM = ColSmem<Real, N, TC>;
     constexpr int T = P::T;
     constexpr int E = N / T;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
+    C* pre0 = sm + SM::FFT;     // state, then the next stage input X
+    C* pre1 = pre0 + SM::PRE;   // accumulator
     if (block_should_exit(a.status)) return;
     const int c = threadIdx.x % TC;
     const int t = threadIdx.x / TC;
     const int ky = blockIdx.x * TC + c;
     const bool valid = ky < a.nyf;
     const int kyc = valid ? ky : 0;
-
-    C x[E];  // spectral values at kx rows i = t + T m of column ky (stage input)
+    const int ldc = a.ldc;
 
     if constexpr (MODE == COL_P1) {
+        const C* __restrict__ src = a.src;
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
-            x[m] = valid ? a.src[(size_t)i * a.ldc + kyc] : cmake<C>(0, 0);
+            if (valid) cp_async_elem(pre0 + i * TC + c, src + (size_t)i * ldc + ky);
+            else pre0[i * TC + c] = cmake<C>(0, 0);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        if (a.col0_out && ky == 0) {
+            // snapshot of the input's column 0 for a later conjugacy step whose
+            // kernel also rewrites the state (AB4 update)
+#pragma unroll
+            for (int m = 0; m < E; ++m) a.col0_out[t + T * m] = pre0[(t + T * m) * TC + c];
         }
     } else {
+        const C* __restrict__ src = a.src;
         C v[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
-            v[m] = valid ? a.src[(size_t)i * a.ldc + kyc] : cmake<C>(0, 0);
+            v[m] = valid ? src[(size_t)i * ldc + kyc] : cmake<C>(0, 0);
+        }
+        // prefetch the epilogue operands while the forward transform runs
+        constexpr bool need_state = (MODE == COL_STAGE || MODE == COL_FINAL);
+        const bool need_acc = (MODE == COL_STAGE && !a.first) || (MODE == COL_FINAL && a.scheme < 2);
+        if constexpr (need_state) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int i = t + T * m;
+                if (valid) {
+                    cp_async_elem(pre0 + i * TC + c, a.state + (size_t)i * ldc + ky);
+                    if (need_acc) cp_async_elem(pre1 + i * TC + c, a.acc + (size_t)i * ldc + ky);
+                } else {
+                    pre0[i * TC + c] = cmake<C>(0, 0);
+                    pre1[i * TC + c] = cmake<C>(0, 0);
+                }
+            }
+            cp_async_commit();
         }
         fft<N, -1, TC>(v, sm, a.tw, t, c);
+        if constexpr (need_state) cp_async_wait_all();
         double bsum = 0.0;
         bool bad = false;
 #pragma unroll
@@ -183,20 +257,18 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
             }
             // forcing (solver.c:1022-1027)
             if (a.has_force && i == a.force_i && ky == a.force_j) r = cadd(r, a.force_val);
-            if (a.rhs_store && valid) a.rhs_store[(size_t)i * a.ldc + ky] = r;
+            if (a.rhs_store && valid) a.rhs_store[(size_t)i * ldc + ky] = r;
             // ForceConjugacy side effect on the state (solver.c:1031, 2096-2103)
             C w = cmake<C>(0, 0);
-            if constexpr (MODE != COL_RHS) {
-                if (valid) w = a.state[(size_t)i * a.ldc + ky];
-            }
+            if constexpr (need_state) w = pre0[i * TC + c];
             if (a.conj_mode && ky == 0 && kx < 0 && valid) {
                 w = cconj(a.conj_src[(size_t)(-kx) * a.conj_stride]);
-                a.state[(size_t)i * a.ldc] = w;
+                a.state[(size_t)i * ldc] = w;
             }
-            if constexpr (MODE != COL_RHS) {
+            if constexpr (need_state) {
                 // linear term of explicit RK4 stages (solver.c:664-684)
                 if (a.lin_stage && k2 != 0) {
-                    const C xs = a.xin ? a.xin[(size_t)i * a.ldc + kyc] : w;
+                    const C xs = a.xin ? a.xin[(size_t)i * ldc + kyc] : w;
                     const double br = lin_bracket(a.lin, (double)k2);
                     if (a.lin_stage == 1) r = cadd(r, cscale(xs, (Real)(a.dt * br)));
                     else r = csub(r, cscale(xs, (Real)br));
@@ -204,23 +276,20 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                 if constexpr (MODE == COL_STAGE) {
                     C acc;
                     if (a.first) acc = cscale(r, (Real)a.b_cur);
-                    else {
-                        acc = a.acc[(size_t)i * a.ldc + kyc];
-                        acc = cadd(acc, cscale(r, (Real)a.b_cur));
-                    }
-                    if (valid) a.acc[(size_t)i * a.ldc + ky] = acc;
+                    else acc = cadd(pre1[i * TC + c], cscale(r, (Real)a.b_cur));
+                    if (valid) a.acc[(size_t)i * ldc + ky] = acc;
                     const Real adt = (Real)(a.dt * a.a_next);
-                    C nx = cadd(w, cscale(r, adt));
-                    x[m] = nx;
+                    const C nx = cadd(w, cscale(r, adt));
+                    pre0[i * TC + c] = nx;
                     if (valid) {
                         if (ky == 0) a.col0_out[i] = nx;
-                        if (a.out) a.out[(size_t)i * a.ldc + ky] = nx;
+                        if (a.out) a.out[(size_t)i * ldc + ky] = nx;
                     }
                 } else {  // COL_FINAL
                     C tot;
                     if (a.scheme >= 2) {
                         // AB4 (solver.c:303-331): 55/24 N_n - 59/24 N_n-1 + 37/24 N_n-2 - 3/8 N_n-3
-                        const size_t q = (size_t)i * a.ldc + kyc;
+                        const size_t q = (size_t)i * ldc + kyc;
                         const C p2 = a.h2[q], p1 = a.h1[q], p0 = a.h0[q];
                         if (a.scheme == 3) {
                             const Real dt = (Real)a.dt;
@@ -233,8 +302,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                                        cscale(p0, (Real)(-3.0 / 8.0)));
                         }
                     } else {
-                        C acc = a.acc[(size_t)i * a.ldc + kyc];
-                        tot = cadd(acc, cscale(r, (Real)a.b_cur));
+                        tot = cadd(pre1[i * TC + c], cscale(r, (Real)a.b_cur));
                     }
                     C wn;
                     if (kx == 0 && ky == 0) {
@@ -244,11 +312,13 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                     } else if (a.scheme == 3) {
                         wn = cadd(w, tot);
                     } else {
+                        // Crank-Nicolson factors (solver.c:853)
                         const double D = a.dt * lin_bracket(a.lin, (double)k2);
-                        wn = cadd(cscale(w, (Real)((2.0 - D) / (2.0 + D))), cscale(tot, (Real)(2.0 * a.dt / (2.0 + D))));
+                        const double rcp = 1.0 / (2.0 + D);
+                        wn = cadd(cscale(w, (Real)((2.0 - D) * rcp)), cscale(tot, (Real)(2.0 * a.dt * rcp)));
                     }
                     if (valid) {
-                        a.state[(size_t)i * a.ldc + ky] = wn;
+                        a.state[(size_t)i * ldc + ky] = wn;
                         const double mag = fabs((double)wn.x) + fabs((double)wn.y);
                         bad |= !isfinite(mag);
                         bsum += (ky == 0 || 2 * ky == N) ? mag : 2.0 * mag;
@@ -268,8 +338,8 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
             if ((threadIdx.x & 31) == 0) {
                 atomicAdd(a.blowup_sum, bsum);
                 if (anybad) atomicOr(a.status, 1);
+                __threadfence();
             }
-            __threadfence();
             __syncthreads();
             if (threadIdx.x == 0) {
                 unsigned int* ticket = reinterpret_cast<unsigned int*>(a.blowup_sum + 1);
@@ -289,36 +359,23 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
         if constexpr (MODE == COL_RHS) return;
     }
 
-    // derived spectra of the stage input and four inverse x-FFTs (solver.c:904-957)
+    // derived spectra of the stage input and four inverse x-FFTs; one copy of
+    // the transform code serves all four fields
     C* outs[4] = {a.f0, a.f1, a.f2, a.f3};
-#pragma unroll
+#pragma unroll 1
     for (int f = 0; f < 4; ++f) {
         C v[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
             const int kx = (i <= N / 2) ? i : i - N;
-            const C X = x[m];
-            if (kx == 0 && ky == 0) {
-                v[m] = cmake<C>(0, 0);
-            } else if (f == 0 || f == 1) {
-                const double inv = 1.0 / (double)(kx * kx + ky * ky);
-                if (f == 0) {
-                    const Real s = (Real)((double)ky * inv);
-                    v[m] = cmake<C>(-s * X.y, s * X.x);
-                } else {
-                    const Real s = (Real)((double)kx * inv);
-                    v[m] = cmake<C>(s * X.y, -s * X.x);
-                }
-            } else {
-                const Real s = (Real)(f == 2 ? kx : ky);
-                v[m] = cmake<C>(-s * X.y, s * X.x);
-            }
+            v[m] = derived(f, kx, ky, pre0[i * TC + c]);
         }
         fft<N, +1, TC>(v, sm, a.tw, t, c);
         if (valid) {
+            C* __restrict__ o = outs[f];
 #pragma unroll
-            for (int m = 0; m < E; ++m) outs[f][(size_t)(t + T * m) * a.ldc + ky] = v[m];
+            for (int m = 0; m < E; ++m) o[(size_t)(t + T * m) * ldc + ky] = v[m];
         }
     }
 }
@@ -337,6 +394,24 @@ struct RowArgs {
     int* status;
 };
 
+// Shared memory of the row pass: FFT exchange buffer, then the WX and WY
+// half rows of the block's TC rows (prefetched with cp.async).
+template <typename Real, int N, int TC>
+struct RowSmem {
+    using C = typename Cx<Real>::T;
+    static constexpr int FFT = SmemLayout<N, TC>::ELEMS;
+    // row pitch: N/2+1 rounded so that the TC rows start in different banks
+    static constexpr int PITCH = ((N / 2 + 1 + 7) / 8) * 8 + (TC >= 8 ? 1 : 8 / TC);
+    static constexpr int PRE = 2 * TC * PITCH;
+    // u and v of pass 0, [2][N][TC] reals, after the prefetch area
+    static constexpr size_t UV_OFFSET = sizeof(C) * (size_t)(FFT + PRE);
+    static constexpr size_t bytes() {
+        size_t a = UV_OFFSET + sizeof(Real) * 2 * (size_t)N * TC;
+        size_t b = sizeof(Real) * (size_t)N * TC;
+        return a > b ? a : b;
+    }
+};
+
 // Row pass.  Block: 2*PAIRS*T threads = TC = 2*PAIRS transforms (one per x row);
 // grid: nrows / (2*PAIRS).  Rows 2p and 2p+1 of the block share one packed
 // forward transform, computed by both of their thread groups.
@@ -348,57 +423,81 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
     constexpr int E = N / T;
     constexpr int TC = 2 * PAIRS;
     using L = SmemLayout<N, TC>;
+    using RS = RowSmem<Real, N, TC>;
+    constexpr int NYF = N / 2 + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
+    C* pre = sm + RS::FFT;  // [field 0/1][row g][PITCH]
     if (block_should_exit(a.status)) return;
     const int g = threadIdx.x % TC;  // row within the block
     const int t = threadIdx.x / TC;
-    const int x = blockIdx.x * TC + g;
-    const C* rowU = a.f0 + (size_t)x * a.ldc;
-    const C* rowV = a.f1 + (size_t)x * a.ldc;
-    const C* rowWX = a.f2 + (size_t)x * a.ldc;
-    const C* rowWY = a.f3 + (size_t)x * a.ldc;
+    const int x0 = blockIdx.x * TC;
+    const int x = x0 + g;
+    // prefetch WX, WY of all TC rows (pass 1) while pass 0 runs
+    for (int q = threadIdx.x; q < 2 * TC * NYF; q += blockDim.x) {
+        const int f = q / (TC * NYF);
+        const int rem = q - f * TC * NYF;
+        const int rg = rem / NYF, y = rem - rg * NYF;
+        const C* base = (f == 0 ? a.f2 : a.f3) + (size_t)(x0 + rg) * a.ldc + y;
+        cp_async_elem(pre + (f * TC + rg) * RS::PITCH + y, base);
+    }
+    cp_async_commit();
 
-    Real u[E], v[E];
+    Real* uv = reinterpret_cast<Real*>(smraw + RS::UV_OFFSET);  // own slots only
+    Real nl[E];
     C z[E];
     // Z1 = U + i V over the full y range (Hermitian extension; DC and Nyquist
     // use the real parts only, as FFTW's c2r does)
-#pragma unroll
+#pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
-        const C* A = pass == 0 ? rowU : rowWX;
-        const C* B = pass == 0 ? rowV : rowWY;
+        if (pass == 0) {
+            const C* __restrict__ A = a.f0 + (size_t)x * a.ldc;
+            const C* __restrict__ B = a.f1 + (size_t)x * a.ldc;
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int y = t + T * m;
-            if (y == 0 || y == N / 2) {
-                z[m] = cmake<C>(A[y].x, B[y].x);
-            } else if (y < N / 2) {
-                const C p = A[y], q = B[y];
-                z[m] = cmake<C>(p.x - q.y, p.y + q.x);
-            } else {
-                const C p = A[N - y], q = B[N - y];
-                z[m] = cmake<C>(p.x + q.y, q.x - p.y);
+            for (int m = 0; m < E; ++m) {
+                const int y = t + T * m;
+                const int yy = (y <= N / 2) ? y : N - y;
+                const C p = A[yy], q = B[yy];
+                if (y == 0 || y == N / 2) z[m] = cmake<C>(p.x, q.x);
+                else if (y < N / 2) z[m] = cmake<C>(p.x - q.y, p.y + q.x);
+                else z[m] = cmake<C>(p.x + q.y, q.x - p.y);
+            }
+        } else {
+            cp_async_wait_all();
+            __syncthreads();
+            const C* A = pre + (0 * TC + g) * RS::PITCH;
+            const C* B = pre + (1 * TC + g) * RS::PITCH;
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int y = t + T * m;
+                const int yy = (y <= N / 2) ? y : N - y;
+                const C p = A[yy], q = B[yy];
+                if (y == 0 || y == N / 2) z[m] = cmake<C>(p.x, q.x);
+                else if (y < N / 2) z[m] = cmake<C>(p.x - q.y, p.y + q.x);
+                else z[m] = cmake<C>(p.x + q.y, q.x - p.y);
             }
         }
         fft<N, +1, TC>(z, sm, a.tw, t, g);
         if (pass == 0) {
 #pragma unroll
             for (int m = 0; m < E; ++m) {
-                u[m] = z[m].x;
-                v[m] = z[m].y;
+                const int q = (t + T * m) * TC + g;
+                uv[q] = z[m].x;
+                uv[N * TC + q] = z[m].y;
             }
         } else {
 #pragma unroll
             for (int m = 0; m < E; ++m) {
                 // n = 1.0 * (u w_x + v w_y)  (solver.c:979-981)
-                u[m] = u[m] * z[m].x + v[m] * z[m].y;
+                const int q = (t + T * m) * TC + g;
+                nl[m] = uv[q] * z[m].x + uv[N * TC + q] * z[m].y;
             }
         }
     }
     // pack rows (2p, 2p+1): zr = n_a + i n_b
     Real* rs = reinterpret_cast<Real*>(smraw);
 #pragma unroll
-    for (int m = 0; m < E; ++m) rs[(t + T * m) * TC + g] = u[m];
+    for (int m = 0; m < E; ++m) rs[(t + T * m) * TC + g] = nl[m];
     __syncthreads();
     const int ga = g & ~1;
 #pragma unroll

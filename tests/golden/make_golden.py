@@ -46,6 +46,10 @@ def cases():
         # reads only the real parts there) and the conjugacy side effect
         "nonherm32_rhs": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, dt=1e-3),
                           ("decaying", 5, 4.0), [("rhs_input", 77), ("w_hat",)]),
+        # Hou-Li filter (integer k/(N/2) as in solver.c:1088) at 32^2 where the
+        # Nyquist row/column are populated; reference built with __DEALIAS_HOU_LI
+        "houli32": ("houli", dict(nx=32, ny=32, nu=5e-4, dealias=abi.DEALIAS_HOU_LI, dt=1e-3),
+                    ("decaying", 8, 6.0, None), [("rhs_state",), ("steps", 10, 1e-3), ("w_hat",)]),
         # adaptive CFL step with the reference's row-index quirk
         "cfl32": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9, dt=1e-3),
                   ("decaying", 6, 4.0), [("cfl", 1e-3), ("steps", 5, 2e-3), ("cfl", 2e-3), ("w_hat",)]),
@@ -56,7 +60,7 @@ def make_ic(spec, n):
     if spec[0] == "tg":
         return initial.taylor_green(n)
     if spec[0] == "decaying":
-        return initial.decaying(n, seed=spec[1], k0=spec[2], dealias="2/3")
+        return initial.decaying(n, seed=spec[1], k0=spec[2], dealias=spec[3] if len(spec) > 3 else "2/3")
     if spec[0] == "noise":
         return initial.noise(n, seed=spec[1], amplitude=1e-3, kolm=True)
     raise ValueError(spec)
