@@ -36,7 +36,7 @@ struct LinOp {
 
 // Out of line: the callers sit in fully unrolled per-element loops, and one
 // shared copy of this code keeps the kernels inside the instruction cache.
-__device__ __noinline__ double pow_general(double x, double p) { return pow(x, p); }
+static __device__ __noinline__ double pow_general(double x, double p) { return pow(x, p); }
 
 __device__ __forceinline__ double powk(double k2, double p, int pint) {
     if (pint != -2147483647 - 1) {

@@ -197,6 +197,30 @@ ns2d_status ns2d_system_measurables(ns2d_handle* h, ns2d_measures* out, double* 
 /* Real-space vorticity [nx][ny] (c2r of the state, normalised). */
 ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
 
+/* The nonlinear term of NonlinearRHSBatch for callers that cannot allocate
+   device memory.  No counterpart in the reference; it exists for code that runs
+   under somebody else's stream capture (cudaMalloc cannot be recorded into a
+   graph), for time loops that cannot afford cudaMalloc's implicit device
+   synchronisation, and for applications whose device memory comes from their
+   own pool.  No handle: the caller passes the parameters and two device arrays
+   in the reference layout, [nx][ny/2+1] complex128 (d_w_hat read, d_rhs
+   written), and the work is queued on cuda_stream (NULL = legacy default).
+   The output equals ns2d_nonlinear_rhs(h, w_hat, rhs) after
+   ns2d_compute_forcing on a handle with the same parameters; the conjugacy
+   side effect on a state does not apply (there is none).  FP64 only.
+   Limit: square grids of 16..NS2D_NOALLOC_MAX_N; larger sizes return
+   NS2D_ERR_UNSUPPORTED before touching the device.  The intermediate fields
+   live in one static device array of NS2D_NOALLOC_SCRATCH_BYTES that every GPU
+   loading the library holds until exit.  All calls on a device share that
+   array, so calls that overlap on the GPU (unordered streams) race.  The first
+   call on each device (and for each grid size) does set-up -- it looks up the
+   array's device address and sets kernel shared-memory limits -- and should
+   come before any stream capture. */
+#define NS2D_NOALLOC_MAX_N 256
+#define NS2D_NOALLOC_SCRATCH_BYTES (16u * (5u * 256u * 129u + 256u))
+ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const double* d_w_hat, double* d_rhs,
+                                       void* cuda_stream);
+
 /* Execution control. */
 ns2d_status ns2d_set_stream(ns2d_handle* h, void* cuda_stream);
 ns2d_status ns2d_get_stream(const ns2d_handle* h, void** cuda_stream);
