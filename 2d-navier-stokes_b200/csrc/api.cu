@@ -44,6 +44,10 @@ struct ns2d_handle {
     int* dstatus = nullptr;    // [0] bits, [1] completed steps
     double2* dio = nullptr;    // staging [nx][nyf] complex128
     double* ddiag = nullptr;   // measurables: DG_N totals + 8 * n_spect spectra
+    double* dpart = nullptr;   // per-block partial bounds of the final column pass
+    double2* cn = nullptr;     // Crank-Nicolson factors per mode ([nx][ldc])
+    double cn_dt = 0.0;        // dt and branch the table was built for
+    int cn_branch = -1;
     // model state kept on the host
     int hyper_flag = 0;
     bool forced = false;
@@ -149,6 +153,7 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.inv_nxny = norm_fac;
     a.status = h->dstatus;
     a.blowup_sum = h->dscal;
+    a.partials = h->dpart;
     a.lin = make_lin(h, branch);
 }
 
@@ -222,6 +227,17 @@ void compute_forcing(ns2d_handle* h, double dt) {
     }
 }
 
+// Rebuild the Crank-Nicolson factor table when dt or the operator branch changed.
+ns2d_status ensure_cn(ns2d_handle* h, double dt, int branch) {
+    if (h->cn_dt == dt && h->cn_branch == branch) return NS2D_OK;
+    cn_table_kernel<<<296, 256, 0, h->stream>>>(h->cn, h->nx, h->nyf, h->ldc, dt, make_lin(h, branch));
+    h->launches++;
+    CKL(h);
+    h->cn_dt = dt;
+    h->cn_branch = branch;
+    return NS2D_OK;
+}
+
 // One RK4 / RK4CN step (RK4Step, Solver/src/solver.c:625-873).  If rk1_out is
 // non-null the stage-1 RHS is stored there (AB4 start-up, solver.c:283).
 template <typename Real>
@@ -269,6 +285,11 @@ ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out) {
             launch_col<Real>(h, COL_STAGE, a);
         } else {
             a.scheme = explicit_rk4 ? 1 : 0;
+            if (!explicit_rk4) {
+                ns2d_status s2 = ensure_cn(h, dt, branch);
+                if (s2) return s2;
+                a.cn = h->cn;
+            }
             launch_col<Real>(h, COL_FINAL, a);
         }
     }
@@ -296,6 +317,11 @@ ns2d_status ab4_update_impl(ns2d_handle* h, double dt) {
     a.conj_src = (const C*)h->col0[0];
     a.conj_stride = 1;
     a.scheme = euler ? 3 : 2;
+    if (!euler) {
+        ns2d_status s2 = ensure_cn(h, dt, branch);
+        if (s2) return s2;
+        a.cn = h->cn;
+    }
     a.h0 = (const C*)h->ab[0];
     a.h1 = (const C*)h->ab[1];
     a.h2 = (const C*)h->ab[2];
@@ -432,7 +458,7 @@ void fill_twiddles(std::vector<Cplx<Real>>& tw, int n) {
 void free_all(ns2d_handle* h) {
     void* ptrs[] = {h->state, h->acc, h->nl, h->f[0], h->f[1], h->f[2], h->f[3], h->tmpfull, h->col0[0], h->col0[1],
                     h->tw, h->rhsbuf, h->ab[0], h->ab[1], h->ab[2], h->ab[3], h->uhat_ref, h->dreal, h->dscal, h->dmax,
-                    h->dstatus, h->dio, h->ddiag};
+                    h->dstatus, h->dio, h->ddiag, h->dpart, h->cn};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -462,6 +488,8 @@ ns2d_status create_impl(ns2d_handle* h) {
     CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(int) * 4, h->stream));
     CK(h, cudaMalloc(&h->dio, sizeof(double2) * (size_t)h->nx * h->nyf));
     CK(h, cudaMalloc(&h->ddiag, sizeof(double) * (DG_N + 8 * (size_t)h->n_spect)));
+    CK(h, cudaMalloc(&h->dpart, sizeof(double) * 4096));
+    CK(h, cudaMalloc(&h->cn, sizeof(double2) * (size_t)h->nx * h->ldc));
     CK(h, cudaFuncSetAttribute((const void*)diag_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(sizeof(double) * (8 * (size_t)h->n_spect + DG_N * 8))));
     std::vector<C> tw;

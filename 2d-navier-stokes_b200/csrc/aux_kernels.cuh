@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_inv_kernel(InvArgs<Real> 
     const int ky = blockIdx.x * TC + c;
     const bool valid = ky < a.nyf;
     const int kyc = valid ? ky : 0;
+    const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
     for (int f = 0; f < a.nf; ++f) {
         const InvField<Real> F = a.f[f];
         C v[E];
@@ -63,7 +64,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_inv_kernel(InvArgs<Real> 
             }
             v[m] = w;
         }
-        fft<N, +1, TC>(v, sm, a.tw, t, c);
+        fft<N, +1, TC>(v, sm, seed, t, c);
         if (valid) {
 #pragma unroll
             for (int m = 0; m < E; ++m) F.dst[(size_t)(t + T * m) * a.ldc + ky] = v[m];
@@ -100,6 +101,7 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_c2r_kernel(RowC2RA
     const int x = blockIdx.x * TC + g;
     const C* rA = a.A + (size_t)x * a.ldc;
     const C* rB = a.B ? a.B + (size_t)x * a.ldc : nullptr;
+    const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
     C z[E];
 #pragma unroll
     for (int m = 0; m < E; ++m) {
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_c2r_kernel(RowC2RA
             z[m] = cmake<C>(p.x + q.y, q.x - p.y);
         }
     }
-    fft<N, +1, TC>(z, sm, a.tw, t, g);
+    fft<N, +1, TC>(z, sm, seed, t, g);
     double mx = 0.0;
 #pragma unroll
     for (int m = 0; m < E; ++m) {

@@ -6,13 +6,15 @@
 
 namespace ns2d {
 
-// Column-tile width (ky columns per block) and row pairs per block, chosen so
-// that blocks have about 128 threads.
+// Column-tile width (ky columns per block) and row pairs per block.  Column
+// accesses fetch TC * 16 B per row, so wider tiles use each row's cache line
+// better; at 512 and 1024 four columns per block measured faster than two
+// (even with fewer blocks than SMs at 1024), so they get TC = 4.
 template <int N>
 struct Shape {
     static constexpr int T = Plan<N>::T;
     static constexpr int TC_RAW = 128 / T < 2 ? 2 : 128 / T;
-    static constexpr int TC = (N == 16) ? 8 : TC_RAW;
+    static constexpr int TC = (N == 16) ? 8 : (N == 512 || N == 1024) ? 4 : TC_RAW;
     static constexpr int PAIRS_RAW = (128 / T) / 2 < 1 ? 1 : (128 / T) / 2;
     static constexpr int PAIRS = PAIRS_RAW > N / 2 ? N / 2 : PAIRS_RAW;
 };

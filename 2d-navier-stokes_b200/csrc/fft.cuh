@@ -145,21 +145,45 @@ struct SmemLayout {
     __device__ __forceinline__ static int slot(int e, int c) { return (e + e / PADR) * TC + c; }
 };
 
-// Twiddle exp(SIGN 2 pi i m / N) from the table tw[m] = exp(-2 pi i m / N).
-template <int SIGN, typename C>
-__device__ __forceinline__ C twiddle(const C* __restrict__ tw, int m) {
-    C w = __ldg(tw + m);
+// Per-thread twiddle seeds.  In every plan T is a multiple of the middle
+// stage's Ns, so a thread's middle-stage butterflies all share k = t mod Ns and
+// its twiddles are powers of one value; the last stage's twiddles are powers of
+// exp(-2 pi i t / N).  The seeds are loaded once per kernel and the powers
+// w^r (r < R) are formed by a multiplication tree of depth log2 R, so the
+// transform issues no table loads of its own.
+template <typename C>
+struct TwSeed {
+    C mid;   // exp(-2 pi i (t mod Ns1) (N / (Ns1 R1)) / N)
+    C last;  // exp(-2 pi i t / N)
+};
+
+template <int N, typename C>
+__device__ __forceinline__ TwSeed<C> twiddle_seeds(const C* __restrict__ tw, int t) {
+    using P = Plan<N>;
+    TwSeed<C> s;
+    constexpr int NS1 = P::R0;
+    s.mid = __ldg(tw + (t % NS1) * (N / (NS1 * P::R1)));
+    s.last = __ldg(tw + t);
+    return s;
+}
+
+// out[r] = w^r for r < R (out[0] unused), with conj(w) for SIGN > 0.
+template <int R, int SIGN, typename C>
+__device__ __forceinline__ void tw_powers(C w, C* out) {
     if constexpr (SIGN > 0) w.y = -w.y;
-    return w;
+    out[1] = w;
+#pragma unroll
+    for (int r = 2; r < R; ++r) out[r] = (r & 1) ? cmul(out[r - 1], w) : cmul(out[r / 2], out[r / 2]);
 }
 
 // Middle stage: reads smem (pattern of the previous stage's writes), writes smem.
 template <int N, int R, int NS, int SIGN, int TC, typename C>
-__device__ __forceinline__ void middle_stage(C* sm, const C* __restrict__ tw, int t, int c) {
+__device__ __forceinline__ void middle_stage(C* sm, C wseed, int t, int c) {
     using P = Plan<N>;
     using L = SmemLayout<N, TC>;
     constexpr int BPT = N / (R * P::T);
     static_assert(BPT * R * P::T == N, "plan");
+    static_assert(P::T % NS == 0, "middle-stage twiddles must depend on t only");
     C v[BPT][R];
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
@@ -168,12 +192,14 @@ __device__ __forceinline__ void middle_stage(C* sm, const C* __restrict__ tw, in
         for (int r = 0; r < R; ++r) v[b][r] = sm[L::slot(j + r * (N / R), c)];
     }
     __syncthreads();
+    C w[R];
+    tw_powers<R, SIGN>(wseed, w);
+    const int k = t % NS;
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
         const int j = t + P::T * b;
-        const int k = j % NS;
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, k * r * (N / (NS * R))));
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], w[r]);
         small_dft<R, SIGN>(v[b]);
         const int base = (j / NS) * NS * R + k;
 #pragma unroll
@@ -186,7 +212,7 @@ __device__ __forceinline__ void middle_stage(C* sm, const C* __restrict__ tw, in
 // sm must hold SmemLayout<N,TC>::ELEMS elements shared by the TC transforms of
 // the block; all threads of the block must call this together.
 template <int N, int SIGN, int TC, typename C>
-__device__ __forceinline__ void fft(C* v, C* sm, const C* __restrict__ tw, int t, int c) {
+__device__ __forceinline__ void fft(C* v, C* sm, const TwSeed<C>& seed, int t, int c) {
     using P = Plan<N>;
     using L = SmemLayout<N, TC>;
     constexpr int E = N / P::T;
@@ -198,18 +224,129 @@ __device__ __forceinline__ void fft(C* v, C* sm, const C* __restrict__ tw, int t
     __syncthreads();
     constexpr int NS1 = P::R0;
     if constexpr (P::S == 3) {
-        middle_stage<N, P::R1, NS1, SIGN, TC>(sm, tw, t, c);
+        middle_stage<N, P::R1, NS1, SIGN, TC>(sm, seed.mid, t, c);
     }
     constexpr int RL = (P::S == 3) ? P::R2 : P::R1;
-    constexpr int NSL = N / RL;
     static_assert(RL == P::R0, "last radix must equal the first");
-    // last stage: j = t, Ns = N / RL = T, outputs at t + r T
+    // last stage: j = t, Ns = N / RL = T, outputs at t + r T, twiddles w^r with
+    // w = exp(SIGN 2 pi i t / N)
 #pragma unroll
     for (int r = 0; r < RL; ++r) v[r] = sm[L::slot(t + r * (N / RL), c)];
+    C w[RL];
+    tw_powers<RL, SIGN>(seed.last, w);
 #pragma unroll
-    for (int r = 1; r < RL; ++r) v[r] = cmul(v[r], twiddle<SIGN>(tw, (t % NSL) * r * (N / (NSL * RL))));
+    for (int r = 1; r < RL; ++r) v[r] = cmul(v[r], w[r]);
     small_dft<RL, SIGN>(v);
     __syncthreads();  // the shared buffer may be reused right after
+}
+
+}  // namespace ns2d
+
+namespace ns2d {
+
+// ---------------------------------------------------------------------------
+// Team transforms.  A team is the T threads of one transform (Plan<N>::T),
+// laid out as whole warps when T >= 32, and it owns a private shared region of
+// B * ROWS elements (one per transform in flight).  Teams synchronise with
+// their own named barrier, so the teams of a block advance independently.
+// ---------------------------------------------------------------------------
+template <int N>
+struct TeamLayout {
+    static constexpr int PADR = Plan<N>::R0;
+    static constexpr int ROWS = N + N / PADR;
+    __device__ __forceinline__ static int slot(int e) { return e + e / PADR; }
+};
+
+template <int T>
+__device__ __forceinline__ void team_sync(int bar) {
+    if constexpr (T >= 32) {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "r"(T) : "memory");
+    } else {
+        __syncwarp();
+    }
+}
+
+// Layout/sync policies for batched transforms.
+// Interleaved: the TC transforms of a block share one padded buffer per batch
+// entry (c fastest), synchronised with the block barrier.
+template <int N, int TC, typename C>
+struct IlvPolicy {
+    C* sm;
+    int c;
+    static constexpr int STRIDE = SmemLayout<N, TC>::ELEMS;
+    __device__ __forceinline__ C& at(int b, int e) const { return sm[b * STRIDE + SmemLayout<N, TC>::slot(e, c)]; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+// Team: private padded regions, named barrier (or warp barrier below 32 threads).
+template <int N, typename C>
+struct TeamPolicy {
+    C* sm;
+    int bar;
+    static constexpr int STRIDE = TeamLayout<N>::ROWS;
+    __device__ __forceinline__ C& at(int b, int e) const { return sm[b * STRIDE + TeamLayout<N>::slot(e)]; }
+    __device__ __forceinline__ void sync() const { team_sync<Plan<N>::T>(bar); }
+};
+
+// B transforms of length N in lockstep.  v[b][m] = x_b[t + T m] in and out.
+// The twiddle powers are shared by the B transforms; one barrier phase serves
+// all of them.
+template <int N, int SIGN, int B, typename C, typename Pol>
+__device__ __forceinline__ void fft_batched(C (&v)[B][N / Plan<N>::T], const Pol& pol, const TwSeed<C>& seed, int t) {
+    using P = Plan<N>;
+    constexpr int T = P::T;
+    constexpr int E = N / T;
+    static_assert(E == P::R0, "first stage must be one butterfly per thread");
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        small_dft<P::R0, SIGN>(v[b]);
+#pragma unroll
+        for (int r = 0; r < P::R0; ++r) pol.at(b, t * P::R0 + r) = v[b][r];
+    }
+    pol.sync();
+    if constexpr (P::S == 3) {
+        constexpr int R = P::R1;
+        constexpr int NS = P::R0;
+        constexpr int BPT = N / (R * T);
+        static_assert(T % NS == 0, "middle-stage twiddles must depend on t only");
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+#pragma unroll
+            for (int bb = 0; bb < BPT; ++bb)
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[b][bb * R + r] = pol.at(b, t + T * bb + r * (N / R));
+        pol.sync();
+        C w[R];
+        tw_powers<R, SIGN>(seed.mid, w);
+        const int k = t % NS;
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+#pragma unroll
+            for (int bb = 0; bb < BPT; ++bb) {
+                const int j = t + T * bb;
+                C* u = &v[b][bb * R];
+#pragma unroll
+                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], w[r]);
+                small_dft<R, SIGN>(u);
+                const int base = (j / NS) * NS * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) pol.at(b, base + r * NS) = u[r];
+            }
+        }
+        pol.sync();
+    }
+    constexpr int RL = (P::S == 3) ? P::R2 : P::R1;
+    static_assert(RL == P::R0, "last radix must equal the first");
+    C w[RL];
+    tw_powers<RL, SIGN>(seed.last, w);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+#pragma unroll
+        for (int r = 0; r < RL; ++r) v[b][r] = pol.at(b, t + r * T);
+#pragma unroll
+        for (int r = 1; r < RL; ++r) v[b][r] = cmul(v[b][r], w[r]);
+        small_dft<RL, SIGN>(v[b]);
+    }
+    pol.sync();  // the buffers may be reused right after
 }
 
 }  // namespace ns2d

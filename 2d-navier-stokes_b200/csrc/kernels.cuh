@@ -99,7 +99,9 @@ struct ColArgs {
     const C* h2;
     int lin_stage;       // 0 none, 1: rhs += dt D X (quirk), 2: rhs -= D X (corrected)
     LinOp lin;
-    double* blowup_sum;  // COL_FINAL: [0] bound accumulator, [1] ticket counter
+    const double2* cn;   // COL_FINAL, CN schemes: per-mode ((2-D)/(2+D), 2dt/(2+D)), stride ldc
+    double* blowup_sum;  // COL_FINAL: [1] holds the ticket counter
+    double* partials;    // COL_FINAL: one partial bound per block
     double inv_nxny;     // 1/(Nx Ny)
     int* status;         // [0] status bits (kernels return early when set), [1] completed steps
 };
@@ -150,14 +152,16 @@ __device__ __forceinline__ void cp_async_elem(C* smem, const C* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Shared memory of the column pass: the FFT exchange buffer, then two
-// [N][TC] staging arrays (state or stage input, and the RK accumulator).
+// Shared memory of the column pass: two FFT exchange buffers (the second one
+// first holds the prefetched RK accumulator), then the [N][TC] staging array
+// of the state, which becomes the next stage input X.
 template <typename Real, int N, int TC>
 struct ColSmem {
     using C = typename Cx<Real>::T;
     static constexpr int FFT = SmemLayout<N, TC>::ELEMS;
     static constexpr int PRE = N * TC;
-    static constexpr size_t bytes() { return sizeof(C) * (size_t)(FFT + 2 * PRE); }
+    static_assert(FFT >= PRE, "accumulator staging must fit the second exchange buffer");
+    static constexpr size_t bytes() { return sizeof(C) * (size_t)(2 * FFT + PRE); }
 };
 
 // Derived spectrum f of the stage input X at (kx, ky) (solver.c:904-957):
@@ -187,8 +191,8 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     constexpr int E = N / T;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
-    C* pre0 = sm + SM::FFT;     // state, then the next stage input X
-    C* pre1 = pre0 + SM::PRE;   // accumulator
+    C* pre1 = sm + SM::FFT;       // accumulator, later the second exchange buffer
+    C* pre0 = sm + 2 * SM::FFT;   // state, then the next stage input X
     if (block_should_exit(a.status)) return;
     const int c = threadIdx.x % TC;
     const int t = threadIdx.x / TC;
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     const bool valid = ky < a.nyf;
     const int kyc = valid ? ky : 0;
     const int ldc = a.ldc;
+    const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
 
     if constexpr (MODE == COL_P1) {
         const C* __restrict__ src = a.src;
@@ -215,11 +220,11 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
         }
     } else {
         const C* __restrict__ src = a.src;
-        C v[E];
+        C v[1][E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
-            v[m] = valid ? src[(size_t)i * ldc + kyc] : cmake<C>(0, 0);
+            v[0][m] = valid ? src[(size_t)i * ldc + kyc] : cmake<C>(0, 0);
         }
         // prefetch the epilogue operands while the forward transform runs
         constexpr bool need_state = (MODE == COL_STAGE || MODE == COL_FINAL);
@@ -238,17 +243,23 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
             }
             cp_async_commit();
         }
-        fft<N, -1, TC>(v, sm, a.tw, t, c);
+        fft_batched<N, -1, 1>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
+        // The epilogue runs as a rolled loop over this thread's elements (one
+        // copy of its code): the transform output is parked in the exchange
+        // buffer, in slots only this thread touches.
+#pragma unroll
+        for (int m = 0; m < E; ++m) sm[(t + T * m) * TC + c] = v[0][m];
         if constexpr (need_state) cp_async_wait_all();
         double bsum = 0.0;
         bool bad = false;
-#pragma unroll
+#pragma unroll 4
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
+            const int q = i * TC + c;
             const int kx = (i <= N / 2) ? i : i - N;
             const int k2 = kx * kx + ky * ky;
             // normalisation and zero mean (solver.c:998-1013)
-            C r = (kx == 0 && ky == 0) ? cmake<C>(0, 0) : cscale(v[m], a.norm2);
+            C r = (kx == 0 && ky == 0) ? cmake<C>(0, 0) : cscale(sm[q], a.norm2);
             // dealiasing (solver.c:1039-1099)
             if (a.dealias == 0) {
                 if ((double)k2 >= (double)a.kmax_sqr || (a.kolm && kx == 0)) r = cmake<C>(0, 0);
@@ -260,7 +271,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
             if (a.rhs_store && valid) a.rhs_store[(size_t)i * ldc + ky] = r;
             // ForceConjugacy side effect on the state (solver.c:1031, 2096-2103)
             C w = cmake<C>(0, 0);
-            if constexpr (need_state) w = pre0[i * TC + c];
+            if constexpr (need_state) w = pre0[q];
             if (a.conj_mode && ky == 0 && kx < 0 && valid) {
                 w = cconj(a.conj_src[(size_t)(-kx) * a.conj_stride]);
                 a.state[(size_t)i * ldc] = w;
@@ -276,11 +287,11 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                 if constexpr (MODE == COL_STAGE) {
                     C acc;
                     if (a.first) acc = cscale(r, (Real)a.b_cur);
-                    else acc = cadd(pre1[i * TC + c], cscale(r, (Real)a.b_cur));
+                    else acc = cadd(pre1[q], cscale(r, (Real)a.b_cur));
                     if (valid) a.acc[(size_t)i * ldc + ky] = acc;
                     const Real adt = (Real)(a.dt * a.a_next);
                     const C nx = cadd(w, cscale(r, adt));
-                    pre0[i * TC + c] = nx;
+                    pre0[q] = nx;
                     if (valid) {
                         if (ky == 0) a.col0_out[i] = nx;
                         if (a.out) a.out[(size_t)i * ldc + ky] = nx;
@@ -289,8 +300,8 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                     C tot;
                     if (a.scheme >= 2) {
                         // AB4 (solver.c:303-331): 55/24 N_n - 59/24 N_n-1 + 37/24 N_n-2 - 3/8 N_n-3
-                        const size_t q = (size_t)i * ldc + kyc;
-                        const C p2 = a.h2[q], p1 = a.h1[q], p0 = a.h0[q];
+                        const size_t g = (size_t)i * ldc + kyc;
+                        const C p2 = a.h2[g], p1 = a.h1[g], p0 = a.h0[g];
                         if (a.scheme == 3) {
                             const Real dt = (Real)a.dt;
                             tot = cadd(cadd(cadd(cscale(r, dt * (Real)(55.0 / 24.0)), cscale(p2, dt * (Real)(-59.0 / 24.0))),
@@ -302,7 +313,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                                        cscale(p0, (Real)(-3.0 / 8.0)));
                         }
                     } else {
-                        tot = cadd(pre1[i * TC + c], cscale(r, (Real)a.b_cur));
+                        tot = cadd(pre1[q], cscale(r, (Real)a.b_cur));
                     }
                     C wn;
                     if (kx == 0 && ky == 0) {
@@ -312,10 +323,9 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                     } else if (a.scheme == 3) {
                         wn = cadd(w, tot);
                     } else {
-                        // Crank-Nicolson factors (solver.c:853)
-                        const double D = a.dt * lin_bracket(a.lin, (double)k2);
-                        const double rcp = 1.0 / (2.0 + D);
-                        wn = cadd(cscale(w, (Real)((2.0 - D) * rcp)), cscale(tot, (Real)(2.0 * a.dt * rcp)));
+                        // Crank-Nicolson factors (solver.c:853), from the table
+                        const double2 f = a.cn[(size_t)i * ldc + kyc];
+                        wn = cadd(cscale(w, (Real)f.x), cscale(tot, (Real)f.y));
                     }
                     if (valid) {
                         a.state[(size_t)i * ldc + ky] = wn;
@@ -326,29 +336,47 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
                 }
             }
         }
+        // the next transform's first stage writes other threads' parked slots
+        __syncthreads();
         if constexpr (MODE == COL_FINAL) {
             // SystemCheck (solver.c:2301-2326) without a transform: max|w(x)| is
             // bounded by sum|w_hat|/(Nx Ny) over the full spectrum.  Status bit 1:
             // non-finite state; bit 2: bound >= 1e100 (the host then evaluates
-            // max|w| exactly).  The last block to finish (atomic ticket, no
-            // waiting) checks the total and resets the accumulator.
+            // max|w| exactly).  Each block writes its partial sum; the last block
+            // to finish (atomic ticket, no waiting) adds them up.
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
             const unsigned anybad = __ballot_sync(0xffffffffu, bad);
-            if ((threadIdx.x & 31) == 0) {
-                atomicAdd(a.blowup_sum, bsum);
+            double* wsum = reinterpret_cast<double*>(smraw);  // parked slots are free again
+            __shared__ int is_last;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            const int nwarps = (int)(blockDim.x >> 5);
+            if (lane == 0) {
+                wsum[warp] = bsum;
                 if (anybad) atomicOr(a.status, 1);
-                __threadfence();
             }
             __syncthreads();
+            unsigned int* ticket = reinterpret_cast<unsigned int*>(a.blowup_sum + 1);
             if (threadIdx.x == 0) {
-                unsigned int* ticket = reinterpret_cast<unsigned int*>(a.blowup_sum + 1);
-                const unsigned int done = atomicAdd(ticket, 1u);
-                if (done == gridDim.x - 1) {
-                    __threadfence();
-                    const double total = atomicAdd(a.blowup_sum, 0.0);
+                double tot = 0.0;
+                for (int w = 0; w < nwarps; ++w) tot += wsum[w];
+                a.partials[blockIdx.x] = tot;
+                __threadfence();
+                is_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+            }
+            __syncthreads();
+            if (is_last) {
+                __threadfence();
+                double v = 0.0;
+                for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) v += __ldcg(a.partials + b);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) wsum[nwarps + warp] = v;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    double total = 0.0;
+                    for (int w = 0; w < nwarps; ++w) total += wsum[nwarps + w];
                     if (!(total * a.inv_nxny < 1e100)) atomicOr(a.status, 2);
-                    *a.blowup_sum = 0.0;
                     *ticket = 0u;
                     atomicAdd(a.status + 1, 1);  // completed steps
                     __threadfence();
@@ -359,23 +387,29 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
         if constexpr (MODE == COL_RHS) return;
     }
 
-    // derived spectra of the stage input and four inverse x-FFTs; one copy of
-    // the transform code serves all four fields
+    // derived spectra of the stage input and four inverse x-FFTs, two at a
+    // time (one copy of the transform code serves both pairs)
     C* outs[4] = {a.f0, a.f1, a.f2, a.f3};
 #pragma unroll 1
-    for (int f = 0; f < 4; ++f) {
-        C v[E];
+    for (int fp = 0; fp < 4; fp += 2) {
+        C v[2][E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
             const int kx = (i <= N / 2) ? i : i - N;
-            v[m] = derived(f, kx, ky, pre0[i * TC + c]);
+            const C X = pre0[i * TC + c];
+            v[0][m] = derived(fp, kx, ky, X);
+            v[1][m] = derived(fp + 1, kx, ky, X);
         }
-        fft<N, +1, TC>(v, sm, a.tw, t, c);
+        fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
         if (valid) {
-            C* __restrict__ o = outs[f];
+            C* __restrict__ o0 = outs[fp];
+            C* __restrict__ o1 = outs[fp + 1];
 #pragma unroll
-            for (int m = 0; m < E; ++m) o[(size_t)(t + T * m) * ldc + ky] = v[m];
+            for (int m = 0; m < E; ++m) {
+                o0[(size_t)(t + T * m) * ldc + ky] = v[0][m];
+                o1[(size_t)(t + T * m) * ldc + ky] = v[1][m];
+            }
         }
     }
 }
@@ -394,27 +428,22 @@ struct RowArgs {
     int* status;
 };
 
-// Shared memory of the row pass: FFT exchange buffer, then the WX and WY
-// half rows of the block's TC rows (prefetched with cp.async).
+// Shared memory of the row pass: per row (one team of T threads), two padded
+// exchange regions; after the inverse transforms the second region holds the
+// row's product n(x, y) for the packed forward transform.
 template <typename Real, int N, int TC>
 struct RowSmem {
     using C = typename Cx<Real>::T;
-    static constexpr int FFT = SmemLayout<N, TC>::ELEMS;
-    // row pitch: N/2+1 rounded so that the TC rows start in different banks
-    static constexpr int PITCH = ((N / 2 + 1 + 7) / 8) * 8 + (TC >= 8 ? 1 : 8 / TC);
-    static constexpr int PRE = 2 * TC * PITCH;
-    // u and v of pass 0, [2][N][TC] reals, after the prefetch area
-    static constexpr size_t UV_OFFSET = sizeof(C) * (size_t)(FFT + PRE);
-    static constexpr size_t bytes() {
-        size_t a = UV_OFFSET + sizeof(Real) * 2 * (size_t)N * TC;
-        size_t b = sizeof(Real) * (size_t)N * TC;
-        return a > b ? a : b;
-    }
+    static constexpr int TEAM = 2 * TeamLayout<N>::ROWS;
+    static_assert(TeamLayout<N>::ROWS * sizeof(C) >= N * sizeof(Real), "product must fit a region");
+    static constexpr size_t bytes() { return sizeof(C) * (size_t)TEAM * TC; }
 };
 
-// Row pass.  Block: 2*PAIRS*T threads = TC = 2*PAIRS transforms (one per x row);
-// grid: nrows / (2*PAIRS).  Rows 2p and 2p+1 of the block share one packed
-// forward transform, computed by both of their thread groups.
+// Row pass.  Block: TC = 2*PAIRS rows, one team of T threads per row (whole
+// warps when T >= 32); grid: nrows / TC.  Each team runs its row's two inverse
+// transforms together; rows 2p and 2p+1 then share one packed forward
+// transform, done by team 2p alone when teams are whole warps (team 2p+1
+// leaves) and by both teams, each keeping its half, below a warp.
 template <typename Real, int N, int PAIRS>
 __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Real> a) {
     using C = typename Cx<Real>::T;
@@ -422,110 +451,100 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
     constexpr int T = P::T;
     constexpr int E = N / T;
     constexpr int TC = 2 * PAIRS;
-    using L = SmemLayout<N, TC>;
+    using TL = TeamLayout<N>;
     using RS = RowSmem<Real, N, TC>;
-    constexpr int NYF = N / 2 + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    C* pre = sm + RS::FFT;  // [field 0/1][row g][PITCH]
     if (block_should_exit(a.status)) return;
-    const int g = threadIdx.x % TC;  // row within the block
-    const int t = threadIdx.x / TC;
-    const int x0 = blockIdx.x * TC;
-    const int x = x0 + g;
-    // prefetch WX, WY of all TC rows (pass 1) while pass 0 runs
-    for (int q = threadIdx.x; q < 2 * TC * NYF; q += blockDim.x) {
-        const int f = q / (TC * NYF);
-        const int rem = q - f * TC * NYF;
-        const int rg = rem / NYF, y = rem - rg * NYF;
-        const C* base = (f == 0 ? a.f2 : a.f3) + (size_t)(x0 + rg) * a.ldc + y;
-        cp_async_elem(pre + (f * TC + rg) * RS::PITCH + y, base);
-    }
-    cp_async_commit();
+    const int g = threadIdx.x / T;  // row (team) within the block
+    const int t = threadIdx.x % T;
+    const int x = blockIdx.x * TC + g;
+    C* region = reinterpret_cast<C*>(smraw) + (size_t)g * RS::TEAM;
+    const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
+    const TeamPolicy<N, C> pol{region, 1 + g};
 
-    Real* uv = reinterpret_cast<Real*>(smraw + RS::UV_OFFSET);  // own slots only
-    Real nl[E];
-    C z[E];
-    // Z1 = U + i V over the full y range (Hermitian extension; DC and Nyquist
-    // use the real parts only, as FFTW's c2r does)
-#pragma unroll 1
-    for (int pass = 0; pass < 2; ++pass) {
-        if (pass == 0) {
-            const C* __restrict__ A = a.f0 + (size_t)x * a.ldc;
-            const C* __restrict__ B = a.f1 + (size_t)x * a.ldc;
+    // Z1 = U + i V and Z2 = WX + i WY over the full y range (Hermitian
+    // extension; DC and Nyquist use the real parts only, as FFTW's c2r does)
+    C v[2][E];
+    {
+        const C* __restrict__ U = a.f0 + (size_t)x * a.ldc;
+        const C* __restrict__ V = a.f1 + (size_t)x * a.ldc;
+        const C* __restrict__ WX = a.f2 + (size_t)x * a.ldc;
+        const C* __restrict__ WY = a.f3 + (size_t)x * a.ldc;
 #pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const int y = t + T * m;
-                const int yy = (y <= N / 2) ? y : N - y;
-                const C p = A[yy], q = B[yy];
-                if (y == 0 || y == N / 2) z[m] = cmake<C>(p.x, q.x);
-                else if (y < N / 2) z[m] = cmake<C>(p.x - q.y, p.y + q.x);
-                else z[m] = cmake<C>(p.x + q.y, q.x - p.y);
-            }
-        } else {
-            cp_async_wait_all();
-            __syncthreads();
-            const C* A = pre + (0 * TC + g) * RS::PITCH;
-            const C* B = pre + (1 * TC + g) * RS::PITCH;
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const int y = t + T * m;
-                const int yy = (y <= N / 2) ? y : N - y;
-                const C p = A[yy], q = B[yy];
-                if (y == 0 || y == N / 2) z[m] = cmake<C>(p.x, q.x);
-                else if (y < N / 2) z[m] = cmake<C>(p.x - q.y, p.y + q.x);
-                else z[m] = cmake<C>(p.x + q.y, q.x - p.y);
-            }
-        }
-        fft<N, +1, TC>(z, sm, a.tw, t, g);
-        if (pass == 0) {
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const int q = (t + T * m) * TC + g;
-                uv[q] = z[m].x;
-                uv[N * TC + q] = z[m].y;
-            }
-        } else {
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                // n = 1.0 * (u w_x + v w_y)  (solver.c:979-981)
-                const int q = (t + T * m) * TC + g;
-                nl[m] = uv[q] * z[m].x + uv[N * TC + q] * z[m].y;
+        for (int m = 0; m < E; ++m) {
+            const int y = t + T * m;
+            const int yy = (y <= N / 2) ? y : N - y;
+            const C p0 = U[yy], q0 = V[yy], p1 = WX[yy], q1 = WY[yy];
+            if (y == 0 || y == N / 2) {
+                v[0][m] = cmake<C>(p0.x, q0.x);
+                v[1][m] = cmake<C>(p1.x, q1.x);
+            } else if (y < N / 2) {
+                v[0][m] = cmake<C>(p0.x - q0.y, p0.y + q0.x);
+                v[1][m] = cmake<C>(p1.x - q1.y, p1.y + q1.x);
+            } else {
+                v[0][m] = cmake<C>(p0.x + q0.y, q0.x - p0.y);
+                v[1][m] = cmake<C>(p1.x + q1.y, q1.x - p1.y);
             }
         }
     }
-    // pack rows (2p, 2p+1): zr = n_a + i n_b
-    Real* rs = reinterpret_cast<Real*>(smraw);
+    fft_batched<N, +1, 2>(v, pol, seed, t);
+    // n = 1.0 * (u w_x + v w_y)  (solver.c:979-981), parked for the packing
+    Real* nl_own = reinterpret_cast<Real*>(region + TL::ROWS);
 #pragma unroll
-    for (int m = 0; m < E; ++m) rs[(t + T * m) * TC + g] = nl[m];
+    for (int m = 0; m < E; ++m) nl_own[t + T * m] = v[0][m].x * v[1][m].x + v[0][m].y * v[1][m].y;
     __syncthreads();
     const int ga = g & ~1;
+    if constexpr (T >= 32) {
+        if (g & 1) return;  // the pair's packed transform is done by the even team
+    }
+    const Real* na = reinterpret_cast<const Real*>(reinterpret_cast<C*>(smraw) + (size_t)ga * RS::TEAM + TL::ROWS);
+    const Real* nb = reinterpret_cast<const Real*>(reinterpret_cast<C*>(smraw) + (size_t)(ga + 1) * RS::TEAM + TL::ROWS);
+    C z[1][E];
 #pragma unroll
     for (int m = 0; m < E; ++m) {
         const int y = t + T * m;
-        z[m] = cmake<C>(rs[y * TC + ga], rs[y * TC + ga + 1]);
+        z[0][m] = cmake<C>(na[y], nb[y]);
     }
-    __syncthreads();
-    fft<N, -1, TC>(z, sm, a.tw, t, g);
+    fft_batched<N, -1, 1>(z, pol, seed, t);
     // split: X_a = (Z_k + conj Z_{N-k})/2, X_b = (Z_k - conj Z_{N-k})/(2i)
-    if ((g & 1) == 0) {
 #pragma unroll
-        for (int m = 0; m < E; ++m) sm[L::slot(t + T * m, g >> 1)] = z[m];
-    }
-    __syncthreads();
-    const int p = g >> 1;
-    C* dst = a.nl + (size_t)x * a.ldc;
+    for (int m = 0; m < E; ++m) region[TL::slot(t + T * m)] = z[0][m];
+    pol.sync();
+    C* dst_a = a.nl + (size_t)(blockIdx.x * TC + ga) * a.ldc;
+    C* dst_b = dst_a + a.ldc;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
         const int k = t + T * m;
         if (k <= N / 2) {
-            const C zk = sm[L::slot(k, p)];
-            const C zm = sm[L::slot((N - k) & (N - 1), p)];
-            C r;
-            if ((g & 1) == 0) r = cmake<C>((Real)0.5 * (zk.x + zm.x), (Real)0.5 * (zk.y - zm.y));
-            else r = cmake<C>((Real)0.5 * (zk.y + zm.y), (Real)0.5 * (zm.x - zk.x));
-            dst[k] = r;
+            const C zk = region[TL::slot(k)];
+            const C zm = region[TL::slot((N - k) & (N - 1))];
+            const C ra = cmake<C>((Real)0.5 * (zk.x + zm.x), (Real)0.5 * (zk.y - zm.y));
+            const C rb = cmake<C>((Real)0.5 * (zk.y + zm.y), (Real)0.5 * (zm.x - zk.x));
+            if constexpr (T >= 32) {
+                dst_a[k] = ra;
+                dst_b[k] = rb;
+            } else {
+                if (g & 1) dst_b[k] = rb;
+                else dst_a[k] = ra;
+            }
         }
+    }
+}
+
+// Crank-Nicolson factors per mode for the current dt and operator branch:
+// cn = ((2 - D)/(2 + D), 2 dt/(2 + D)), D = dt * bracket(|k|^2) (solver.c:839-853).
+static __global__ void cn_table_kernel(double2* cn, int nx, int nyf, int ldc, double dt, LinOp lin) {
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), ky = (int)(q % nyf);
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        const double k2 = (double)(kx * kx + ky * ky);
+        double2 f = make_double2(0.0, 0.0);
+        if (kx != 0 || ky != 0) {
+            const double D = dt * lin_bracket(lin, k2);
+            f = make_double2((2.0 - D) / (2.0 + D), (2.0 * dt) / (2.0 + D));
+        }
+        cn[(size_t)i * ldc + ky] = f;
     }
 }
 
