@@ -14,6 +14,7 @@
 #include "../../include/ns2d.h"
 #include "diag.cuh"
 #include "engine.cuh"
+#include "host_common.h"
 
 using namespace ns2d;
 
@@ -89,38 +90,18 @@ ns2d_status fail(ns2d_handle* h, ns2d_status s, const std::string& msg) {
         if (e_ != cudaSuccess) return fail((h), NS2D_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
     } while (0)
 
-bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+// Branch of the linear operator for this evaluation (see host_common.h).
+int resolve_branch(ns2d_handle* h, bool latch) { return ns2d::resolve_branch(h->hyper_flag, h->p.ekmn_drag_flag, latch); }
 
-int int_exponent(double p) {
-    double r = std::nearbyint(p);
-    if (r == p && std::fabs(r) <= 64.0) return (int)r;
-    return INT_MIN;
-}
-
-// Branch of the linear operator for this evaluation (Solver/src/solver.c:839-856).
-// With the reference's `=` typo (quirk) the third test assigns the flag first.
-int resolve_branch(ns2d_handle* h, bool latch) {
-    const int drag = h->p.ekmn_drag_flag;
-    if (h->hyper_flag == 1 && drag == 1) return 1;
-    if (h->hyper_flag != 1 && drag == 1) return 2;
-    if (latch) h->hyper_flag = 1;
-    if (h->hyper_flag == 1 && drag != 1) return 3;
-    return 4;
-}
-
-LinOp make_lin(const ns2d_handle* h, int branch) {
-    LinOp L;
-    L.nu = h->p.nu;
-    L.alpha = h->p.ekmn_alpha;
-    L.hp = h->p.hyper_visc_pow;
-    L.dp = h->p.ekmn_drag_pow;
-    L.branch = branch;
-    L.hp_int = int_exponent(L.hp);
-    L.dp_int = int_exponent(L.dp);
-    return L;
-}
+LinOp make_lin(const ns2d_handle* h, int branch) { return make_lin_params(h->p, branch); }
 
 bool quirk(const ns2d_handle* h, int bit) { return (h->p.quirks & bit) != 0; }
+
+int col_tc(int n) {
+    int tc = 0;
+    with_size<double>(n, [&](auto L) { tc = decltype(L)::S::TC; });
+    return tc;
+}
 
 template <typename Real>
 using Cplx = typename Cx<Real>::T;
@@ -154,6 +135,8 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.status = h->dstatus;
     a.blowup_sum = h->dscal;
     a.partials = h->dpart;
+    a.final_tail = 1;
+    a.ntiles = (h->nyf + col_tc(h->nx) - 1) / col_tc(h->nx);
     a.lin = make_lin(h, branch);
 }
 

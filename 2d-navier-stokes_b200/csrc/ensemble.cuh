@@ -1,0 +1,132 @@
+// ensemble.cuh -- many independent trajectories of uneven grid sizes advanced
+// together: one launch per pass covers every member.  A launch walks a list
+// of work items (member, tile) with a persistent grid; each item runs the same
+// column or row body as the single-trajectory kernels, instantiated for the
+// member's grid size.  All bodies use 128-thread blocks, so one launch can mix
+// sizes.
+#pragma once
+#include "kernels.cuh"
+
+namespace ns2d {
+
+// Tile shapes of the ensemble kernels: 128 threads for every size.
+template <int N>
+struct EnsShape {
+    static constexpr int T = Plan<N>::T;
+    static constexpr int TC = 128 / T;          // columns per column tile
+    static constexpr int PAIRS = 128 / (2 * T);  // row pairs per row block
+    static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= 64");
+};
+
+#define NS2D_ENS_SIZES(X) X(64) X(128) X(256) X(512) X(1024)
+
+template <typename Real>
+struct EnsMember {
+    ColArgs<Real> col;                    // member pointers and per-size constants
+    RowArgs<Real> row;
+    typename Cx<Real>::T* col0[2];        // column 0 of successive stage inputs
+    int n;
+    int col_tiles, row_blocks;
+};
+
+struct EnsItem {
+    int member;
+    int tile;
+};
+
+// Per-launch stage parameters shared by all members.
+struct EnsStage {
+    double dt, a_next, b_cur;
+    int first, scheme, conj_quirk, stage;  // stage 1..4; 0 = P1 of the step
+    LinOp lin;
+    int* status;
+};
+
+template <typename Real>
+__device__ __forceinline__ void ens_apply_stage(ColArgs<Real>& a, const EnsMember<Real>& mb, const EnsStage& st) {
+    a.dt = st.dt;
+    a.a_next = st.a_next;
+    a.b_cur = st.b_cur;
+    a.first = st.first;
+    a.scheme = st.scheme;
+    a.lin = st.lin;
+    a.final_tail = 0;
+    a.status = st.status;
+    if (st.stage >= 1) {
+        // a.src is the member's product spectrum (set at creation)
+        a.conj_mode = (st.conj_quirk || st.stage == 1) ? 1 : 0;
+        if (st.stage == 1) {
+            a.conj_src = a.state;
+            a.conj_stride = a.ldc;
+        } else {
+            a.conj_src = mb.col0[(st.stage - 1) & 1];
+            a.conj_stride = 1;
+        }
+        a.col0_out = mb.col0[st.stage & 1];
+    } else {
+        a.src = a.state;
+        a.col0_out = nullptr;
+    }
+}
+
+template <typename Real, int MODE>
+__global__ void __launch_bounds__(128) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
+                                                      const EnsItem* __restrict__ items, int nitems, EnsStage st) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (block_should_exit(st.status)) return;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const EnsItem item = items[it];
+        const EnsMember<Real>& mb = members[item.member];
+        ColArgs<Real> a = mb.col;
+        ens_apply_stage(a, mb, st);
+        switch (mb.n) {
+#define NS2D_ENS_COL(NN)                                                         \
+    case NN:                                                                     \
+        col_body<Real, NN, EnsShape<NN>::TC, MODE>(a, item.tile, smraw);         \
+        break;
+            NS2D_ENS_SIZES(NS2D_ENS_COL)
+#undef NS2D_ENS_COL
+            default: break;
+        }
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
+                                                      const EnsItem* __restrict__ items, int nitems, int* status) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (block_should_exit(status)) return;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const EnsItem item = items[it];
+        const EnsMember<Real>& mb = members[item.member];
+        switch (mb.n) {
+#define NS2D_ENS_ROW(NN)                                                         \
+    case NN:                                                                     \
+        row_body<Real, NN, EnsShape<NN>::PAIRS>(mb.row, item.tile, smraw);       \
+        break;
+            NS2D_ENS_SIZES(NS2D_ENS_ROW)
+#undef NS2D_ENS_ROW
+            default: break;
+        }
+    }
+}
+
+template <typename Real>
+struct EnsSmem {
+    static size_t col() {
+        size_t m = 0;
+#define NS2D_ENS_CS(NN) m = m > ColSmem<Real, NN, EnsShape<NN>::TC>::bytes() ? m : ColSmem<Real, NN, EnsShape<NN>::TC>::bytes();
+        NS2D_ENS_SIZES(NS2D_ENS_CS)
+#undef NS2D_ENS_CS
+        return m;
+    }
+    static size_t row() {
+        size_t m = 0;
+#define NS2D_ENS_RS(NN) m = m > RowSmem<Real, NN, 2 * EnsShape<NN>::PAIRS>::bytes() ? m : RowSmem<Real, NN, 2 * EnsShape<NN>::PAIRS>::bytes();
+        NS2D_ENS_SIZES(NS2D_ENS_RS)
+#undef NS2D_ENS_RS
+        return m;
+    }
+};
+
+}  // namespace ns2d

@@ -103,6 +103,8 @@ struct ColArgs {
     double* blowup_sum;  // COL_FINAL: [1] holds the ticket counter
     double* partials;    // COL_FINAL: one partial bound per block
     double inv_nxny;     // 1/(Nx Ny)
+    int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
+    int ntiles;          // number of column tiles of this field
     int* status;         // [0] status bits (kernels return early when set), [1] completed steps
 };
 
@@ -180,23 +182,23 @@ __device__ __forceinline__ C derived(int f, int kx, int ky, C X) {
     return (f == 1) ? cmake<C>(s * X.y, -s * X.x) : cmake<C>(-s * X.y, s * X.x);
 }
 
-// Column pass.  Grid: ceil(nyf / TC) blocks; block: T * TC threads, thread
-// (t, c) with c = threadIdx.x % TC.  Dynamic shared memory: ColSmem::bytes().
+// Column pass on tile `tile` (ky columns tile*TC .. tile*TC+TC-1), by the T*TC
+// threads of a block, thread (t, c) with c = threadIdx.x % TC.  Shared memory:
+// ColSmem::bytes().  Ends with the block synchronised (the shared memory may be
+// reused for another tile).
 template <typename Real, int N, int TC, int MODE>
-__global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
+__device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw) {
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
     using SM = ColSmem<Real, N, TC>;
     constexpr int T = P::T;
     constexpr int E = N / T;
-    extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
     C* pre1 = sm + SM::FFT;       // accumulator, later the second exchange buffer
     C* pre0 = sm + 2 * SM::FFT;   // state, then the next stage input X
-    if (block_should_exit(a.status)) return;
     const int c = threadIdx.x % TC;
     const int t = threadIdx.x / TC;
-    const int ky = blockIdx.x * TC + c;
+    const int ky = tile * TC + c;
     const bool valid = ky < a.nyf;
     const int kyc = valid ? ky : 0;
     const int ldc = a.ldc;
@@ -339,6 +341,12 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
         // the next transform's first stage writes other threads' parked slots
         __syncthreads();
         if constexpr (MODE == COL_FINAL) {
+            if (!a.final_tail) {
+                // ensemble form: only the non-finite check
+                if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(a.status, 1);
+                __syncthreads();
+                return;
+            }
             // SystemCheck (solver.c:2301-2326) without a transform: max|w(x)| is
             // bounded by sum|w_hat|/(Nx Ny) over the full spectrum.  Status bit 1:
             // non-finite state; bit 2: bound >= 1e100 (the host then evaluates
@@ -360,15 +368,15 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
             if (threadIdx.x == 0) {
                 double tot = 0.0;
                 for (int w = 0; w < nwarps; ++w) tot += wsum[w];
-                a.partials[blockIdx.x] = tot;
+                a.partials[tile] = tot;
                 __threadfence();
-                is_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+                is_last = (atomicAdd(ticket, 1u) == (unsigned int)a.ntiles - 1);
             }
             __syncthreads();
             if (is_last) {
                 __threadfence();
                 double v = 0.0;
-                for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) v += __ldcg(a.partials + b);
+                for (int b = threadIdx.x; b < a.ntiles; b += blockDim.x) v += __ldcg(a.partials + b);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                 if (lane == 0) wsum[nwarps + warp] = v;
@@ -414,6 +422,14 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     }
 }
 
+// Column pass of one field.  Grid: ceil(nyf / TC) blocks; block: T * TC threads.
+template <typename Real, int N, int TC, int MODE>
+__global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (block_should_exit(a.status)) return;
+    col_body<Real, N, TC, MODE>(a, blockIdx.x, smraw);
+}
+
 template <typename Real>
 struct RowArgs {
     using C = typename Cx<Real>::T;
@@ -445,7 +461,7 @@ struct RowSmem {
 // transform, done by team 2p alone when teams are whole warps (team 2p+1
 // leaves) and by both teams, each keeping its half, below a warp.
 template <typename Real, int N, int PAIRS>
-__global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Real> a) {
+__device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, unsigned char* smraw) {
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
     constexpr int T = P::T;
@@ -453,11 +469,9 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
     constexpr int TC = 2 * PAIRS;
     using TL = TeamLayout<N>;
     using RS = RowSmem<Real, N, TC>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    if (block_should_exit(a.status)) return;
     const int g = threadIdx.x / T;  // row (team) within the block
     const int t = threadIdx.x % T;
-    const int x = blockIdx.x * TC + g;
+    const int x = rblock * TC + g;
     C* region = reinterpret_cast<C*>(smraw) + (size_t)g * RS::TEAM;
     const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
     const TeamPolicy<N, C> pol{region, 1 + g};
@@ -494,9 +508,9 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
     for (int m = 0; m < E; ++m) nl_own[t + T * m] = v[0][m].x * v[1][m].x + v[0][m].y * v[1][m].y;
     __syncthreads();
     const int ga = g & ~1;
-    if constexpr (T >= 32) {
-        if (g & 1) return;  // the pair's packed transform is done by the even team
-    }
+    bool active = true;
+    if constexpr (T >= 32) active = (g & 1) == 0;  // the pair's packed transform is done by the even team
+    if (active) {
     const Real* na = reinterpret_cast<const Real*>(reinterpret_cast<C*>(smraw) + (size_t)ga * RS::TEAM + TL::ROWS);
     const Real* nb = reinterpret_cast<const Real*>(reinterpret_cast<C*>(smraw) + (size_t)(ga + 1) * RS::TEAM + TL::ROWS);
     C z[1][E];
@@ -510,7 +524,7 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
 #pragma unroll
     for (int m = 0; m < E; ++m) region[TL::slot(t + T * m)] = z[0][m];
     pol.sync();
-    C* dst_a = a.nl + (size_t)(blockIdx.x * TC + ga) * a.ldc;
+    C* dst_a = a.nl + (size_t)(rblock * TC + ga) * a.ldc;
     C* dst_b = dst_a + a.ldc;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
@@ -529,6 +543,15 @@ __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Rea
             }
         }
     }
+    }  // active
+    __syncthreads();  // the shared memory may be reused for another row block
+}
+
+template <typename Real, int N, int PAIRS>
+__global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Real> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (block_should_exit(a.status)) return;
+    row_body<Real, N, PAIRS>(a, blockIdx.x, smraw);
 }
 
 // Crank-Nicolson factors per mode for the current dt and operator branch:

@@ -7,5 +7,6 @@ inputs.
 from . import abi
 from ._lib import NS2DError, load, LIB_PATH
 from .solver import Solver
+from .ensemble import Ensemble
 
-__all__ = ["abi", "Solver", "NS2DError", "load", "LIB_PATH"]
+__all__ = ["abi", "Solver", "Ensemble", "NS2DError", "load", "LIB_PATH"]

@@ -221,6 +221,33 @@ ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
 ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const double* d_w_hat, double* d_rhs,
                                        void* cuda_stream);
 
+/* ---- Batched ensembles -----------------------------------------------------
+   Independent trajectories of possibly different square grid sizes (64..1024)
+   advanced together: every pass of a step is one launch for all members, and
+   the step is replayed from a captured CUDA graph.  The reference has no
+   counterpart inside the solver; it runs parameter sweeps as separate
+   processes (run_solver.py:270-292).  Members share all parameters except the
+   grid size; RK4CN or RK4, FP64 or FP32.  The ensemble's non-finite check
+   replaces SystemCheck's bound. */
+typedef struct ns2d_ensemble ns2d_ensemble;
+ns2d_status ns2d_ensemble_create(const ns2d_params* base, int32_t n_members, const int32_t* sizes,
+                                 ns2d_ensemble** out);
+ns2d_status ns2d_ensemble_destroy(ns2d_ensemble* e);
+const char* ns2d_ensemble_last_error(const ns2d_ensemble* e);
+int64_t ns2d_ensemble_launch_count(const ns2d_ensemble* e);
+ns2d_status ns2d_ensemble_set_w_hat(ns2d_ensemble* e, int32_t member, const double* w_hat);
+ns2d_status ns2d_ensemble_get_w_hat(ns2d_ensemble* e, int32_t member, double* w_hat);
+ns2d_status ns2d_ensemble_step_n(ns2d_ensemble* e, int32_t nsteps, double dt);
+ns2d_status ns2d_ensemble_step_async(ns2d_ensemble* e, int32_t nsteps, double dt);
+ns2d_status ns2d_ensemble_check(ns2d_ensemble* e);
+/* Totals of ComputeSystemMeasurables for one member, flux terms set to 0. */
+ns2d_status ns2d_ensemble_measurables(ns2d_ensemble* e, int32_t member, ns2d_measures* out);
+/* Autotuner: picks the persistent grid of the column and row passes (1..8
+   blocks per SM) by timing steps at dt.  It advances the members. */
+ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, int32_t* row_grid);
+ns2d_status ns2d_ensemble_set_grids(ns2d_ensemble* e, int32_t col_grid, int32_t row_grid);
+ns2d_status ns2d_ensemble_set_stream(ns2d_ensemble* e, void* cuda_stream);
+
 /* Execution control. */
 ns2d_status ns2d_set_stream(ns2d_handle* h, void* cuda_stream);
 ns2d_status ns2d_get_stream(const ns2d_handle* h, void** cuda_stream);

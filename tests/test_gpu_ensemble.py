@@ -1,0 +1,78 @@
+"""Batched ensembles on the GPU (BASELINE config 4 shape, scaled down).
+
+FP64 members must reproduce single-trajectory handles (same per-column and
+per-row arithmetic; only the launch grouping differs), to 1e-14 of max|w_hat|.
+FP32 members: enstrophy within 1e-5 (relative) of the FP64 oracle after 100
+RK4CN steps, the target stated for the batched form."""
+import numpy as np
+import pytest
+
+from _util import rel_err
+from ns2d import Ensemble, Solver, abi, initial
+from pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _ics(sizes, seed0=0):
+    rng = np.random.default_rng(1234)
+    return [initial.decaying(n, seed=seed0 + m, k0=float(rng.choice([4, 6, 8])) * n / 128.0, dealias="2/3")
+            for m, n in enumerate(sizes)]
+
+
+def test_fp64_ensemble_equals_single_handles():
+    sizes = [64, 128, 64, 256, 512, 128]
+    p = abi.default_params(nu=1e-3, dt=1e-3)
+    ics = _ics(sizes)
+    e = Ensemble(p, sizes)
+    for m, w in enumerate(ics):
+        e.set_w_hat(m, w)
+    e.step_n(12, 1e-3)
+    for m, n in enumerate(sizes):
+        s = Solver(abi.default_params(nx=n, ny=n, nu=1e-3, dt=1e-3))
+        s.set_w_hat(ics[m])
+        s.step_n(12, 1e-3)
+        assert rel_err(e.get_w_hat(m), s.get_w_hat()) <= 1e-14, (m, n)
+        s.close()
+    assert e.launch_count > 0
+    e.close()
+
+
+def test_fp32_ensemble_enstrophy_vs_fp64_oracle():
+    sizes = [128, 256, 128]
+    p = abi.default_params(nu=1e-3, dt=1e-3, precision=abi.FP32)
+    ics = _ics(sizes, seed0=40)
+    e = Ensemble(p, sizes)
+    for m, w in enumerate(ics):
+        e.set_w_hat(m, w)
+    e.step_n(100, 1e-3)
+    for m, n in enumerate(sizes):
+        o = Oracle(abi.default_params(nx=n, ny=n, nu=1e-3, dt=1e-3), threads=8)
+        o.set_w_hat(ics[m])
+        for _ in range(100):
+            o.rk4_step(1e-3)
+        z_ref = initial.enstrophy(o.get_w_hat())
+        z32 = e.measurables(m).enstrophy
+        assert abs(z32 - z_ref) <= 1e-5 * z_ref, (m, n, z32, z_ref)
+    e.close()
+
+
+def test_autotuner_and_graph_replay_keep_results():
+    sizes = [64, 128, 256]
+    p = abi.default_params(nu=1e-3, dt=1e-3)
+    ics = _ics(sizes, seed0=70)
+    e = Ensemble(p, sizes)
+    cg, rg = e.tune(1e-3)
+    assert cg >= 1 and rg >= 1
+    for m, w in enumerate(ics):
+        e.set_w_hat(m, w)
+    e.step_n(6, 1e-3)
+    ref = Ensemble(p, sizes)
+    for m, w in enumerate(ics):
+        ref.set_w_hat(m, w)
+    for _ in range(6):
+        ref.step_n(1, 1e-3)
+    for m in range(len(sizes)):
+        assert rel_err(e.get_w_hat(m), ref.get_w_hat(m)) <= 1e-15
+    e.close()
+    ref.close()
