@@ -1,0 +1,430 @@
+// adjoint.cu -- discrete adjoint of the RK4CN step (checkpointed reverse sweep)
+// behind the ns2d_adjoint_* entry points of include/ns2d.h.
+//
+// The reference has no adjoint; this differentiates its RK4Step with __RK4CN
+// (Solver/src/solver.c:625-873) over NonlinearRHSBatch (solver.c:884-1032).
+//
+// Record: n steps forward from the state, copying w_hat every C steps into a
+// checkpoint.  Reverse: per segment (last first), restore its checkpoint and
+// recompute its steps with the row passes capturing the four real fields of
+// every stage, then run the segment's adjoint steps backwards over them.  One
+// adjoint step is nine launches, the mirror of a forward step:
+//   col START: lambda_x = A lambda'; kappa_4 = b_4 B lambda'; mu_x = IFFT_x(s^2 D kappa_4)
+//   row (stage s): mu = c2r_y(mu_x); products with the stage's fields; two packed r2c_y
+//   col MID (s = 4, 3, 2): L_s from the products; lambda_x += L_s;
+//                          kappa_{s-1} = b_{s-1} B lambda' + a_s dt L_s; mu_x
+//   col END (s = 1): lambda_x += L_1
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ns2d.h"
+#include "adjoint.cuh"
+#include "engine.cuh"
+#include "handle.h"
+
+using namespace ns2d;
+using ns2d::internal::fail;
+
+namespace ns2d {
+
+struct AdjointState {
+    // recorded run
+    bool recorded = false;
+    int nsteps = 0, every = 0;
+    double dt = 0.0;
+    int branch = -1;
+    // buffers
+    void* ckpt = nullptr;  // checkpoints, one field each
+    size_t ckpt_n = 0;
+    void* cap = nullptr;   // captured stage fields: steps x 8 planes of nx*ny complex
+    size_t cap_steps = 0;
+    void* lam[2] = {nullptr, nullptr};
+    void* w_final = nullptr;
+    double* dpart = nullptr;  // per-block partial sums
+    bool ready = false;       // kernel attributes set
+    // event timing of the last reverse sweep (ms): recompute, adjoint
+    double ms_recompute = 0.0, ms_adjoint = 0.0;
+};
+
+}  // namespace ns2d
+
+namespace {
+
+constexpr int kRedBlocks = 296;
+const double kB[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+const double kA[3] = {0.5, 0.5, 1.0};
+
+#define ACK(h, call)                                                                                  \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? NS2D_ERR_NOMEM : NS2D_ERR_CUDA,        \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+template <typename Real, int N>
+struct AdjLaunch {
+    using S = Shape<N>;
+    static constexpr size_t col_smem() { return ColSmem<Real, N, S::TC>::bytes(); }
+    static constexpr size_t row_smem() { return RowSmem<Real, N, 2 * S::PAIRS>::bytes(); }
+    static cudaError_t setup() {
+        cudaError_t e = cudaSuccess;
+        auto set = [&](const void* f, size_t bytes) {
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        };
+        set((const void*)adj_col_kernel<Real, N, S::TC, ADJ_START>, col_smem());
+        set((const void*)adj_col_kernel<Real, N, S::TC, ADJ_MID>, col_smem());
+        set((const void*)adj_col_kernel<Real, N, S::TC, ADJ_END>, col_smem());
+        set((const void*)adj_row_kernel<Real, N, S::PAIRS>, row_smem());
+        return e;
+    }
+    static void col(int mode, const AdjColArgs<Real>& a, cudaStream_t s) {
+        dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
+        switch (mode) {
+            case ADJ_START: adj_col_kernel<Real, N, S::TC, ADJ_START><<<grid, block, col_smem(), s>>>(a); break;
+            case ADJ_MID: adj_col_kernel<Real, N, S::TC, ADJ_MID><<<grid, block, col_smem(), s>>>(a); break;
+            default: adj_col_kernel<Real, N, S::TC, ADJ_END><<<grid, block, col_smem(), s>>>(a); break;
+        }
+    }
+    static void row(const AdjRowArgs<Real>& a, cudaStream_t s) {
+        dim3 grid(N / (2 * S::PAIRS)), block(S::T * 2 * S::PAIRS);
+        adj_row_kernel<Real, N, S::PAIRS><<<grid, block, row_smem(), s>>>(a);
+    }
+};
+
+template <typename Real, typename F>
+bool with_adj_size(int n, F&& f) {
+    return with_size<Real>(n, [&](auto L) { f(AdjLaunch<Real, decltype(L)::SIZE>{}); });
+}
+
+size_t plane_elems(const ns2d_handle* h) { return (size_t)h->nx * h->ny; }
+
+void free_state(AdjointState* a) {
+    void* ptrs[] = {a->ckpt, a->cap, a->lam[0], a->lam[1], a->w_final, a->dpart};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+AdjointState* state_of(ns2d_handle* h) {
+    if (!h->adj) h->adj = new (std::nothrow) AdjointState();
+    return h->adj;
+}
+
+// Buffers for a run of nsteps with checkpoints every `every` steps.
+ns2d_status ensure_buffers(ns2d_handle* h, int nsteps, int every) {
+    AdjointState* a = state_of(h);
+    if (!a) return fail(h, NS2D_ERR_NOMEM, "adjoint state");
+    const size_t nck = (size_t)((nsteps + every - 1) / every);
+    const size_t seg = (size_t)std::min(every, nsteps);
+    if (a->ckpt_n < nck) {
+        if (a->ckpt) cudaFree(a->ckpt);
+        a->ckpt = nullptr;
+        a->ckpt_n = 0;
+        ACK(h, cudaMalloc(&a->ckpt, h->field_bytes * nck));
+        a->ckpt_n = nck;
+    }
+    if (a->cap_steps < seg) {
+        if (a->cap) cudaFree(a->cap);
+        a->cap = nullptr;
+        a->cap_steps = 0;
+        ACK(h, cudaMalloc(&a->cap, h->elem * 8 * plane_elems(h) * seg));
+        a->cap_steps = seg;
+    }
+    for (int k = 0; k < 2; ++k)
+        if (!a->lam[k]) {
+            ACK(h, cudaMalloc(&a->lam[k], h->field_bytes));
+            ACK(h, cudaMemsetAsync(a->lam[k], 0, h->field_bytes, h->stream));
+        }
+    if (!a->w_final) ACK(h, cudaMalloc(&a->w_final, h->field_bytes));
+    if (!a->dpart) ACK(h, cudaMalloc(&a->dpart, sizeof(double) * kRedBlocks));
+    if (!a->ready) {
+        cudaError_t e = cudaSuccess;
+        bool ok = h->fp32 ? with_adj_size<float>(h->nx, [&](auto L) { e = decltype(L)::setup(); })
+                          : with_adj_size<double>(h->nx, [&](auto L) { e = decltype(L)::setup(); });
+        if (!ok) return fail(h, NS2D_ERR_UNSUPPORTED, "grid size");
+        ACK(h, e);
+        a->ready = true;
+    }
+    return NS2D_OK;
+}
+
+ns2d_status validate(ns2d_handle* h) {
+    if (h->p.system != NS2D_NAVIER || h->p.integrator != NS2D_RK4CN)
+        return fail(h, NS2D_ERR_UNSUPPORTED, "the adjoint covers the Navier-Stokes RK4CN step");
+    if (h->p.quirks & NS2D_QUIRK_CONJ_STATE)
+        return fail(h, NS2D_ERR_UNSUPPORTED,
+                    "the adjoint differentiates the corrected ForceConjugacy: clear NS2D_QUIRK_CONJ_STATE");
+    return NS2D_OK;
+}
+
+template <typename Real>
+AdjColArgs<Real> col_common(ns2d_handle* h) {
+    using C = typename Cx<Real>::T;
+    AdjColArgs<Real> a;
+    std::memset(&a, 0, sizeof(a));
+    a.P0 = (const C*)h->f[0];
+    a.P1 = (const C*)h->f[1];
+    a.P2 = (const C*)h->f[2];
+    a.P3 = (const C*)h->f[3];
+    a.cn = h->cn;
+    a.mu = (C*)h->nl;
+    a.tw = (const C*)h->tw;
+    a.ldc = h->ldc;
+    a.nyf = h->nyf;
+    a.norm2 = (Real)std::pow(1.0 / (double)(h->nx * h->ny), 2.0);
+    const int m = (int)(h->nx / 3.0);
+    a.kmax_sqr = m * m;
+    a.dealias = h->p.dealias;
+    a.houli_int = (h->p.quirks & NS2D_QUIRK_HOU_LI_INT) ? 1 : 0;
+    a.kolm = (h->p.forcing == NS2D_FORCING_KOLM) ? 1 : 0;
+    return a;
+}
+
+// One adjoint step over the captured stage fields `cap` (8 planes):
+// lam_x = (step Jacobian)^T lam_p.
+template <typename Real>
+void adjoint_step(ns2d_handle* h, const void* cap, const void* lam_p, void* lam_x, double dt) {
+    using C = typename Cx<Real>::T;
+    AdjColArgs<Real> a = col_common<Real>(h);
+    a.lam_p = (const C*)lam_p;
+    a.lam_x = (C*)lam_x;
+    AdjRowArgs<Real> r;
+    std::memset(&r, 0, sizeof(r));
+    r.mu = (const C*)h->nl;
+    r.P0 = (C*)h->f[0];
+    r.P1 = (C*)h->f[1];
+    r.P2 = (C*)h->f[2];
+    r.P3 = (C*)h->f[3];
+    r.tw = (const C*)h->tw;
+    r.ldc = h->ldc;
+    const size_t plane = plane_elems(h);
+    const C* capc = (const C*)cap;
+    with_adj_size<Real>(h->nx, [&](auto L) {
+        using LL = decltype(L);
+        a.b_next = kB[3];
+        LL::col(ADJ_START, a, h->stream);
+        for (int s = 4; s >= 1; --s) {
+            r.cap_uv = capc + (size_t)(2 * (s - 1)) * plane;
+            r.cap_w = r.cap_uv + plane;
+            LL::row(r, h->stream);
+            if (s > 1) {
+                a.b_next = kB[s - 2];
+                a.adt = kA[s - 2] * dt;
+                LL::col(ADJ_MID, a, h->stream);
+            } else {
+                LL::col(ADJ_END, a, h->stream);
+            }
+        }
+    });
+    h->launches += 9;
+}
+
+// Reverse sweep over the recorded run: adj->lam[0] holds lambda(T) on entry and
+// lambda(0) on return.  The state is left at the recorded final state.
+template <typename Real>
+ns2d_status backward_impl(ns2d_handle* h) {
+    AdjointState* a = h->adj;
+    const size_t plane = plane_elems(h);
+    const size_t step_bytes = h->elem * 8 * plane;
+    const int nck = (a->nsteps + a->every - 1) / a->every;
+    void* lp = a->lam[0];
+    void* lx = a->lam[1];
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    for (auto& e : ev) ACK(h, cudaEventCreate(&e));
+    float t_rec = 0.f, t_adj = 0.f;
+    ns2d_status st = NS2D_OK;
+    for (int seg = nck - 1; seg >= 0 && st == NS2D_OK; --seg) {
+        const int k0 = seg * a->every;
+        const int k1 = std::min(k0 + a->every, a->nsteps);
+        cudaEventRecord(ev[0], h->stream);
+        cudaMemcpyAsync(h->state, (char*)a->ckpt + (size_t)seg * h->field_bytes, h->field_bytes,
+                        cudaMemcpyDeviceToDevice, h->stream);
+        for (int k = k0; k < k1 && st == NS2D_OK; ++k) {
+            h->cap_step = (char*)a->cap + (size_t)(k - k0) * step_bytes;
+            st = internal::rk4_step(h, a->dt);
+        }
+        h->cap_step = nullptr;
+        if (st) break;
+        if (h->cn_dt != a->dt || h->cn_branch != a->branch) {
+            st = fail(h, NS2D_ERR_STATE, "operator branch changed between record and reverse sweep");
+            break;
+        }
+        cudaEventRecord(ev[1], h->stream);
+        for (int k = k1 - 1; k >= k0; --k) {
+            adjoint_step<Real>(h, (const char*)a->cap + (size_t)(k - k0) * step_bytes, lp, lx, a->dt);
+            std::swap(lp, lx);
+        }
+        cudaEventRecord(ev[2], h->stream);
+        cudaEventSynchronize(ev[2]);
+        float m1 = 0.f, m2 = 0.f;
+        cudaEventElapsedTime(&m1, ev[0], ev[1]);
+        cudaEventElapsedTime(&m2, ev[1], ev[2]);
+        t_rec += m1;
+        t_adj += m2;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st) return st;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("adjoint launch: ") + cudaGetErrorString(e));
+    if (lp != a->lam[0]) ACK(h, cudaMemcpyAsync(a->lam[0], lp, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    ACK(h, cudaMemcpyAsync(h->state, a->w_final, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    a->ms_recompute = t_rec;
+    a->ms_adjoint = t_adj;
+    return internal::check_status(h);
+}
+
+ns2d_status backward(ns2d_handle* h) {
+    if (!h->adj || !h->adj->recorded) return fail(h, NS2D_ERR_STATE, "no recorded run: call ns2d_adjoint_record first");
+    return h->fp32 ? backward_impl<float>(h) : backward_impl<double>(h);
+}
+
+// J(state) into *value, its W-gradient into `lam` (internal layout) when non-null.
+template <typename Real>
+ns2d_status objective_impl(ns2d_handle* h, int kind, double* value, void* lam) {
+    using C = typename Cx<Real>::T;
+    AdjointState* a = h->adj;
+    const double cz = 4.0 * M_PI * M_PI * 0.5 / std::pow((double)h->nx * (double)h->ny, 2.0);
+    adj_objective_kernel<Real><<<kRedBlocks, 256, 0, h->stream>>>((const C*)h->state, (C*)lam, h->nx, h->nyf, h->ldc,
+                                                                   cz, kind == NS2D_OBJ_PALINSTROPHY ? 1 : 0, a->dpart);
+    h->launches++;
+    ACK(h, cudaGetLastError());
+    double part[kRedBlocks];
+    ACK(h, cudaMemcpyAsync(part, a->dpart, sizeof(part), cudaMemcpyDeviceToHost, h->stream));
+    ACK(h, cudaStreamSynchronize(h->stream));
+    double tot = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b) tot += part[b];
+    *value = tot;
+    return NS2D_OK;
+}
+
+ns2d_status record(ns2d_handle* h, int nsteps, double dt, int every) {
+    ns2d_status s = validate(h);
+    if (s) return s;
+    if (nsteps < 1 || every < 1 || !(dt > 0.0)) return fail(h, NS2D_ERR_INVALID, "nsteps, checkpoint interval and dt must be positive");
+    if ((s = ensure_buffers(h, nsteps, every))) return s;
+    AdjointState* a = h->adj;
+    a->recorded = false;
+    for (int k = 0; k < nsteps; ++k) {
+        if (k % every == 0)
+            ACK(h, cudaMemcpyAsync((char*)a->ckpt + (size_t)(k / every) * h->field_bytes, h->state, h->field_bytes,
+                                   cudaMemcpyDeviceToDevice, h->stream));
+        if ((s = internal::rk4_step(h, dt))) return s;
+    }
+    if ((s = internal::check_status(h))) return s;
+    ACK(h, cudaMemcpyAsync(a->w_final, h->state, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    a->nsteps = nsteps;
+    a->every = every;
+    a->dt = dt;
+    a->branch = h->cn_branch;
+    a->recorded = true;
+    return NS2D_OK;
+}
+
+}  // namespace
+
+namespace ns2d {
+namespace internal {
+
+void adjoint_free(ns2d_handle* h) {
+    if (!h->adj) return;
+    free_state(h->adj);
+    delete h->adj;
+    h->adj = nullptr;
+}
+
+}  // namespace internal
+}  // namespace ns2d
+
+extern "C" {
+
+ns2d_status ns2d_adjoint_record(ns2d_handle* h, int32_t nsteps, double dt, int32_t checkpoint_every) {
+    if (!h) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    return record(h, nsteps, dt, checkpoint_every);
+}
+
+ns2d_status ns2d_objective(ns2d_handle* h, int32_t kind, double* value, double* d_grad) {
+    if (!h || !value || (kind != NS2D_OBJ_ENSTROPHY && kind != NS2D_OBJ_PALINSTROPHY)) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    ns2d_status s = ensure_buffers(h, 1, 1);
+    if (s) return s;
+    void* lam = d_grad ? h->adj->lam[1] : nullptr;
+    s = h->fp32 ? objective_impl<float>(h, kind, value, lam) : objective_impl<double>(h, kind, value, lam);
+    if (s || !d_grad) return s;
+    return internal::unpack_out(h, lam, (double2*)d_grad);
+}
+
+ns2d_status ns2d_adjoint_backward_device(ns2d_handle* h, const double* d_lam_T, double* d_lam_0) {
+    if (!h || !d_lam_T || !d_lam_0) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    if (!h->adj || !h->adj->recorded) return fail(h, NS2D_ERR_STATE, "no recorded run: call ns2d_adjoint_record first");
+    ns2d_status s = internal::pack_in(h, (const double2*)d_lam_T, h->adj->lam[0]);
+    if (s) return s;
+    if ((s = backward(h))) return s;
+    return internal::unpack_out(h, h->adj->lam[0], (double2*)d_lam_0);
+}
+
+ns2d_status ns2d_adjoint_backward(ns2d_handle* h, const double* lam_T, double* lam_0) {
+    if (!h || !lam_T || !lam_0) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    if (!h->adj || !h->adj->recorded) return fail(h, NS2D_ERR_STATE, "no recorded run: call ns2d_adjoint_record first");
+    const size_t bytes = sizeof(double2) * (size_t)h->nx * h->nyf;
+    ACK(h, cudaMemcpyAsync(h->dio, lam_T, bytes, cudaMemcpyHostToDevice, h->stream));
+    ns2d_status s = internal::pack_in(h, h->dio, h->adj->lam[0]);
+    if (s) return s;
+    if ((s = backward(h))) return s;
+    if ((s = internal::unpack_out(h, h->adj->lam[0], h->dio))) return s;
+    ACK(h, cudaMemcpyAsync(lam_0, h->dio, bytes, cudaMemcpyDeviceToHost, h->stream));
+    ACK(h, cudaStreamSynchronize(h->stream));
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_adjoint_gradient(ns2d_handle* h, int32_t nsteps, double dt, int32_t checkpoint_every, int32_t kind,
+                                  double* value, double* grad) {
+    if (!h || !value || !grad || (kind != NS2D_OBJ_ENSTROPHY && kind != NS2D_OBJ_PALINSTROPHY)) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    ns2d_status s = record(h, nsteps, dt, checkpoint_every);
+    if (s) return s;
+    s = h->fp32 ? objective_impl<float>(h, kind, value, h->adj->lam[0])
+                : objective_impl<double>(h, kind, value, h->adj->lam[0]);
+    if (s) return s;
+    if ((s = backward(h))) return s;
+    if ((s = internal::unpack_out(h, h->adj->lam[0], h->dio))) return s;
+    ACK(h, cudaMemcpyAsync(grad, h->dio, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyDeviceToHost, h->stream));
+    ACK(h, cudaStreamSynchronize(h->stream));
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_recompute, double* ms_adjoint) {
+    if (!h || !h->adj) return NS2D_ERR_INVALID;
+    if (ms_recompute) *ms_recompute = h->adj->ms_recompute;
+    if (ms_adjoint) *ms_adjoint = h->adj->ms_adjoint;
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_wdot_device(ns2d_handle* h, const double* d_a, const double* d_b, double* value) {
+    if (!h || !d_a || !d_b || !value) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    ns2d_status s = ensure_buffers(h, 1, 1);
+    if (s) return s;
+    // the packed complex128 arrays are read as-is: nyf = ldc for this reduction
+    adj_wdot_kernel<double><<<kRedBlocks, 256, 0, h->stream>>>((const double2*)d_a, (const double2*)d_b, h->nx, h->nyf,
+                                                               h->nyf, h->adj->dpart);
+    h->launches++;
+    ACK(h, cudaGetLastError());
+    double part[kRedBlocks];
+    ACK(h, cudaMemcpyAsync(part, h->adj->dpart, sizeof(part), cudaMemcpyDeviceToHost, h->stream));
+    ACK(h, cudaStreamSynchronize(h->stream));
+    double tot = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b) tot += part[b];
+    *value = tot;
+    return NS2D_OK;
+}
+
+}  // extern "C"

@@ -14,56 +14,10 @@
 #include "../../include/ns2d.h"
 #include "diag.cuh"
 #include "engine.cuh"
+#include "handle.h"
 #include "host_common.h"
 
 using namespace ns2d;
-
-struct ns2d_handle {
-    ns2d_params p{};
-    int nx = 0, ny = 0, nyf = 0, ldc = 0;
-    bool fp32 = false;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own = nullptr;  // stream created by ns2d_create
-    std::string err;
-    int64_t launches = 0;
-    size_t elem = 0;         // bytes per complex element
-    size_t field_bytes = 0;  // nx * ldc * elem
-    // device buffers
-    void* state = nullptr;
-    void* acc = nullptr;
-    void* nl = nullptr;
-    void* f[4] = {nullptr, nullptr, nullptr, nullptr};
-    void* tmpfull = nullptr;  // explicit-RK4 stage input / standalone RHS input
-    void* col0[2] = {nullptr, nullptr};
-    void* tw = nullptr;
-    void* rhsbuf = nullptr;
-    void* ab[4] = {nullptr, nullptr, nullptr, nullptr};  // AB4 ring: [0..2] history, [3] next
-    void* uhat_ref = nullptr;  // persistent u_hat in the reference layout (CFL / VEL paths)
-    double* dreal = nullptr;   // [nx][ny] real-space output
-    double* dscal = nullptr;   // [0] bound accumulator, [1] ticket
-    unsigned long long* dmax = nullptr;
-    int* dstatus = nullptr;    // [0] bits, [1] completed steps
-    double2* dio = nullptr;    // staging [nx][nyf] complex128
-    double* ddiag = nullptr;   // measurables: DG_N totals + 8 * n_spect spectra
-    double* dpart = nullptr;   // per-block partial bounds of the final column pass
-    double2* cn = nullptr;     // Crank-Nicolson factors per mode ([nx][ldc])
-    double cn_dt = 0.0;        // dt and branch the table was built for
-    int cn_branch = -1;
-    // model state kept on the host
-    int hyper_flag = 0;
-    bool forced = false;
-    int force_i = 0, force_j = 0;
-    double fre = 0.0, fim = 0.0;
-    double w_max_init = 0.0, min_dt = 10.0, max_dt = 1e-10;
-    int n_spect = 0;
-    int ab_count = 0;
-    // optional per-launch event timing
-    bool timing = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_open;
-    double t_ms[5] = {0, 0, 0, 0, 0};
-    int64_t t_n[5] = {0, 0, 0, 0, 0};
-};
 
 namespace {
 
@@ -143,7 +97,7 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
 template <typename Real>
 RowArgs<Real> row_args(ns2d_handle* h) {
     using C = Cplx<Real>;
-    RowArgs<Real> r;
+    RowArgs<Real> r{};
     r.f0 = (const C*)h->f[0];
     r.f1 = (const C*)h->f[1];
     r.f2 = (const C*)h->f[2];
@@ -193,10 +147,17 @@ void launch_col(ns2d_handle* h, int mode, const ColArgs<Real>& a) {
     TimedLaunch t(h, mode == COL_STAGE ? 1 : mode == COL_FINAL ? 2 : 0);
     with_size<Real>(h->nx, [&](auto L) { decltype(L)::col(mode, a, h->stream); });
 }
+// Row pass of stage `stage` (1..4); with a capture target set, the stage's real
+// fields go to planes 2(stage-1) and 2(stage-1)+1 of it.
 template <typename Real>
-void launch_row(ns2d_handle* h) {
+void launch_row(ns2d_handle* h, int stage = 0) {
     TimedLaunch t(h, 3);
     RowArgs<Real> r = row_args<Real>(h);
+    if (h->cap_step && stage >= 1) {
+        const size_t plane = (size_t)h->nx * h->ny;
+        r.cap_uv = (Cplx<Real>*)h->cap_step + (size_t)(2 * (stage - 1)) * plane;
+        r.cap_w = r.cap_uv + plane;
+    }
     with_size<Real>(h->nx, [&](auto L) { decltype(L)::row(r, h->stream); });
 }
 
@@ -244,7 +205,7 @@ ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out) {
     a.src = (const C*)h->state;
     launch_col<Real>(h, COL_P1, a);
     for (int s = 1; s <= 4; ++s) {
-        launch_row<Real>(h);
+        launch_row<Real>(h, s);
         fill_common<Real>(h, a, branch);
         a.src = (const C*)h->nl;
         a.dt = dt;
@@ -616,6 +577,20 @@ ns2d_status measurables_impl(ns2d_handle* h, ns2d_measures* out, double* spectra
 
 }  // namespace
 
+namespace ns2d {
+namespace internal {
+
+ns2d_status fail(ns2d_handle* h, ns2d_status s, const std::string& msg) { return ::fail(h, s, msg); }
+ns2d_status rk4_step(ns2d_handle* h, double dt) { return DISPATCH(h, rk4_step_impl, h, dt, nullptr); }
+ns2d_status check_status(ns2d_handle* h) { return ::check_status(h); }
+ns2d_status pack_in(ns2d_handle* h, const double2* d_src, void* dst) { return DISPATCH(h, ::pack_in, h, d_src, dst); }
+ns2d_status unpack_out(ns2d_handle* h, const void* src, double2* d_dst) {
+    return DISPATCH(h, ::unpack_out, h, src, d_dst);
+}
+
+}  // namespace internal
+}  // namespace ns2d
+
 extern "C" {
 
 int ns2d_abi_version(void) { return NS2D_ABI_VERSION; }
@@ -709,6 +684,7 @@ ns2d_status ns2d_destroy(ns2d_handle* h) {
     if (!h) return NS2D_ERR_INVALID;
     cudaSetDevice(h->p.device);
     cudaStreamSynchronize(h->stream);
+    internal::adjoint_free(h);
     free_all(h);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     for (auto& e : h->ev_open) {

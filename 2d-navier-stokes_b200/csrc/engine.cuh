@@ -23,6 +23,7 @@ template <typename Real, int N>
 struct Launch {
     using C = typename Cx<Real>::T;
     using S = Shape<N>;
+    static constexpr int SIZE = N;
     static constexpr size_t col_smem() { return ColSmem<Real, N, S::TC>::bytes(); }
     static constexpr size_t row_smem() { return RowSmem<Real, N, 2 * S::PAIRS>::bytes(); }
     static constexpr size_t inv_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }

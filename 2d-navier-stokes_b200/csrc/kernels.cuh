@@ -442,6 +442,8 @@ struct RowArgs {
     int ldc;
     int nrows;
     int* status;
+    C* cap_uv;    // optional capture of the real fields: (u, v) and (w_x, w_y) as
+    C* cap_w;     // complex pairs, [x][y] (adjoint stage recomputation); null = off
 };
 
 // Shared memory of the row pass: per row (one team of T threads), two padded
@@ -502,6 +504,15 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
         }
     }
     fft_batched<N, +1, 2>(v, pol, seed, t);
+    if (a.cap_uv) {
+        C* __restrict__ cu = a.cap_uv + (size_t)x * N;
+        C* __restrict__ cw = a.cap_w + (size_t)x * N;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            cu[t + T * m] = v[0][m];
+            cw[t + T * m] = v[1][m];
+        }
+    }
     // n = 1.0 * (u w_x + v w_y)  (solver.c:979-981), parked for the packing
     Real* nl_own = reinterpret_cast<Real*>(region + TL::ROWS);
 #pragma unroll

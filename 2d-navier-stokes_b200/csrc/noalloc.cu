@@ -143,7 +143,7 @@ extern "C" ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const do
     a.norm2 = std::pow(1.0 / (double)(n * n), 2.0);
     with_small_size(n, [&](auto L) { decltype(L)::col(COL_P1, a, st); });
 
-    RowArgs<double> r;
+    RowArgs<double> r{};
     r.f0 = f[0];
     r.f1 = f[1];
     r.f2 = f[2];

@@ -22,6 +22,7 @@ DEALIAS_23, DEALIAS_HOU_LI = 0, 1
 FORCING_NONE, FORCING_KOLM, FORCING_ZERO = 0, 1, 2
 FP64, FP32 = 0, 1
 MAX_VORT, MAX_VEL, MAX_VORT_FOUR = 0, 1, 2
+OBJ_ENSTROPHY, OBJ_PALINSTROPHY = 0, 1
 
 QUIRK_CONJ_STATE = 1 << 0
 QUIRK_HYPER_LATCH = 1 << 1

@@ -163,6 +163,44 @@ class Solver:
     def synchronize(self):
         self._ck(self.L.ns2d_synchronize(self.h))
 
+    # discrete adjoint (W-gradients: dJ = sum_j c_j Re(conj(g_j) dw_j))
+    def adjoint_record(self, nsteps, dt, checkpoint_every=50):
+        """Advance nsteps RK4CN steps keeping checkpoints for adjoint_backward."""
+        self._ck(self.L.ns2d_adjoint_record(self.h, nsteps, dt, checkpoint_every))
+
+    def adjoint_backward(self, lam_T):
+        """(dw(T)/dw(0))^T lam_T over the recorded run (host arrays)."""
+        lam_T = np.ascontiguousarray(lam_T, np.complex128)
+        out = self._spec()
+        self._ck(self.L.ns2d_adjoint_backward(self.h, _ptr(lam_T.view(np.float64)), _ptr(out.view(np.float64))))
+        return out
+
+    def adjoint_backward_device(self, d_lam_T, d_lam_0):
+        self._ck(self.L.ns2d_adjoint_backward_device(self.h, C.c_void_p(d_lam_T), C.c_void_p(d_lam_0)))
+
+    def objective(self, kind=abi.OBJ_ENSTROPHY, d_grad=None):
+        v = C.c_double()
+        self._ck(self.L.ns2d_objective(self.h, kind, C.byref(v), C.c_void_p(d_grad) if d_grad else None))
+        return v.value
+
+    def adjoint_gradient(self, nsteps, dt, checkpoint_every=50, kind=abi.OBJ_ENSTROPHY):
+        """J(w(T)) and dJ/dw(0) from the current state (the state ends at w(T))."""
+        g = self._spec()
+        v = C.c_double()
+        self._ck(self.L.ns2d_adjoint_gradient(self.h, nsteps, dt, checkpoint_every, kind, C.byref(v),
+                                              _ptr(g.view(np.float64))))
+        return v.value, g
+
+    def adjoint_times(self):
+        a, b = C.c_double(), C.c_double()
+        self._ck(self.L.ns2d_adjoint_times(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def wdot_device(self, d_a, d_b):
+        v = C.c_double()
+        self._ck(self.L.ns2d_wdot_device(self.h, C.c_void_p(d_a), C.c_void_p(d_b), C.byref(v)))
+        return v.value
+
     @property
     def launch_count(self):
         return self.L.ns2d_launch_count(self.h)

@@ -221,6 +221,47 @@ ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
 ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const double* d_w_hat, double* d_rhs,
                                        void* cuda_stream);
 
+/* ---- Discrete adjoint ------------------------------------------------------
+   Gradient of a final-time functional J(w(T)) with respect to the initial
+   vorticity for n fixed-dt RK4CN steps (RK4Step, solver.c:625-873, over
+   NonlinearRHSBatch, solver.c:884-1032).  No counterpart in the reference,
+   whose extreme-enstrophy and max-palinstrophy searches (MAX_PALIN,
+   solver.c:1775-1853) read their initial conditions from files.
+
+   Gradients use the half-spectrum inner product
+       <a, b>_W = sum_j c_j Re(conj(a_j) b_j),  c_j = 1 on ky = 0 and ky = ny/2, 2 else,
+   so dJ = <g, dw0>_W for every Hermitian perturbation dw0.  Arrays are the
+   reference layout [nx][ny/2+1] complex128.  The adjoint covers the
+   Navier-Stokes RK4CN step with NS2D_QUIRK_CONJ_STATE clear (the corrected
+   ForceConjugacy, the identity on Hermitian states); other integrators and that
+   quirk return NS2D_ERR_UNSUPPORTED.  The handle's precision applies to the
+   adjoint too; J and inner products are accumulated in FP64. */
+typedef enum ns2d_objective_kind {
+    NS2D_OBJ_ENSTROPHY = 0,    /* Z = 4 pi^2 0.5/(nx ny)^2 sum_j c_j |w_j|^2 (sys_msr.c:190-227, 356-363) */
+    NS2D_OBJ_PALINSTROPHY = 1  /* P = same with |k|^2 |w_j|^2                                              */
+} ns2d_objective_kind;
+
+/* Advance nsteps RK4CN steps of dt from the state, keeping a copy of w_hat
+   every checkpoint_every steps for ns2d_adjoint_backward (memory: one field per
+   checkpoint plus checkpoint_every steps x 8 real fields for the recomputed
+   stages). */
+ns2d_status ns2d_adjoint_record(ns2d_handle* h, int32_t nsteps, double dt, int32_t checkpoint_every);
+/* Reverse sweep over the recorded run: lam_0 = (dw(T)/dw(0))^T lam_T in the W
+   inner product.  Segments are recomputed from their checkpoints; the state is
+   left at w(T).  Host and device-pointer forms. */
+ns2d_status ns2d_adjoint_backward(ns2d_handle* h, const double* lam_T, double* lam_0);
+ns2d_status ns2d_adjoint_backward_device(ns2d_handle* h, const double* d_lam_T, double* d_lam_0);
+/* J(state) (ns2d_objective_kind) and, when d_grad != NULL, its W-gradient
+   (device array). */
+ns2d_status ns2d_objective(ns2d_handle* h, int32_t kind, double* value, double* d_grad);
+/* The whole gradient: record, J(w(T)), reverse sweep; grad (host) = dJ/dw(0). */
+ns2d_status ns2d_adjoint_gradient(ns2d_handle* h, int32_t nsteps, double dt, int32_t checkpoint_every,
+                                  int32_t kind, double* value, double* grad);
+/* Device time (ms) of the last reverse sweep: stage recomputation, adjoint steps. */
+ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_recompute, double* ms_adjoint);
+/* <a, b>_W of two device arrays, accumulated in FP64. */
+ns2d_status ns2d_wdot_device(ns2d_handle* h, const double* d_a, const double* d_b, double* value);
+
 /* ---- Batched ensembles -----------------------------------------------------
    Independent trajectories of possibly different square grid sizes (64..1024)
    advanced together: every pass of a step is one launch for all members, and

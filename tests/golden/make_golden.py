@@ -127,8 +127,67 @@ def generate(name):
     return len(outs)
 
 
+# ---------------------------------------------------------------------------
+# Tangent-linear fixture for the discrete adjoint: directional derivatives of
+# the final enstrophy and palinstrophy along seeded directions, propagated by a
+# tangent-linear RK4CN step whose RHS derivative is taken from the reference's
+# own NonlinearRHSBatch by polarisation (exact for its quadratic term).
+
+ADJOINT_CASE = dict(nx=32, ny=32, nu=1e-3, quirks=0, dt=2e-3)
+ADJOINT_STEPS = 25
+ADJOINT_DIRS = 4
+
+
+def _adjoint_worker(q):
+    import adjoint_ref as ar
+    from pyoracle import RefSolver
+    p = abi.default_params(**ADJOINT_CASE)
+    n, dt = p.nx, p.dt
+    ref = RefSolver(p, "rk4cn")
+    rhs = ref.nonlinear_rhs
+    model = ar.Model(n, ar.bracket_for(p))
+    tl = ar.tl_rhs_polar(rhs)
+    w0 = initial.decaying(n, seed=21, k0=4.0, dealias="2/3")
+    dirs = [ar.random_field(n, 100 + i, kmax=n / 3.0, scale=np.abs(w0).max()) for i in range(ADJOINT_DIRS)]
+    traj = []
+    w = w0
+    for _ in range(ADJOINT_STEPS):
+        w, X = model.step(w, dt, rhs=rhs)
+        traj.append(X)
+    Z, gZ = model.objective(w, "enstrophy")
+    P, gP = model.objective(w, "palinstrophy")
+    dZ, dP = [], []
+    for d in dirs:
+        dw = d
+        for X in traj:
+            dw = model.step_tl(X, dw, dt, rhs_tl=tl)
+        dZ.append(ar.wdot(gZ, dw))
+        dP.append(ar.wdot(gP, dw))
+    q.put((w0, np.array(dirs), w, Z, P, np.array(dZ), np.array(dP)))
+
+
+def generate_adjoint():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    proc = ctx.Process(target=_adjoint_worker, args=(q,))
+    proc.start()
+    w0, dirs, wT, Z, P, dZ, dP = q.get(timeout=600)
+    proc.join()
+    p = abi.default_params(**ADJOINT_CASE)
+    params = {f: getattr(p, f) for f, _ in abi.Params._fields_}
+    np.savez_compressed(os.path.join(HERE, "adjoint32_tl.npz"), w0=w0, dirs=dirs, wT=wT, Z=Z, P=P, dZ=dZ, dP=dP,
+                        nsteps=ADJOINT_STEPS,
+                        params=np.array([float(params[f]) for f, _ in abi.Params._fields_]),
+                        param_names=np.array([f for f, _ in abi.Params._fields_]))
+
+
 if __name__ == "__main__":
     import pyoracle
     pyoracle.build(ref=True)
+    only = sys.argv[1:]
     for name in cases():
-        print(name, generate(name))
+        if not only or name in only:
+            print(name, generate(name))
+    if not only or "adjoint32_tl" in only:
+        generate_adjoint()
+        print("adjoint32_tl")
