@@ -14,6 +14,10 @@
 //   col MID (s = 4, 3, 2): L_s from the products; lambda_x += L_s;
 //                          kappa_{s-1} = b_{s-1} B lambda' + a_s dt L_s; mu_x
 //   col END (s = 1): lambda_x += L_1
+// The reverse sweep runs on two streams: while the adjoint steps of segment k
+// run on the adjoint stream, the handle's stream recomputes segment k-1 into
+// the other of two capture buffers (one column pass of a 512^2 field covers
+// under half of the SMs, so the two overlap).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,14 +46,19 @@ struct AdjointState {
     // buffers
     void* ckpt = nullptr;  // checkpoints, one field each
     size_t ckpt_n = 0;
-    void* cap = nullptr;   // captured stage fields: steps x 8 planes of nx*ny complex
-    size_t cap_steps = 0;
+    void* cap[2] = {nullptr, nullptr};  // captured stage fields: steps x 8 planes of nx*ny complex
+    size_t cap_steps[2] = {0, 0};
     void* lam[2] = {nullptr, nullptr};
+    void* P[4] = {nullptr, nullptr, nullptr, nullptr};  // adjoint row-pass outputs
+    void* mu = nullptr;                                 // adjoint column-pass output
     void* w_final = nullptr;
     double* dpart = nullptr;  // per-block partial sums
     bool ready = false;       // kernel attributes set
-    // event timing of the last reverse sweep (ms): recompute, adjoint
-    double ms_recompute = 0.0, ms_adjoint = 0.0;
+    cudaStream_t stream = nullptr;  // adjoint stream
+    cudaEvent_t rec_done[2] = {nullptr, nullptr}, adj_done[2] = {nullptr, nullptr}, join = nullptr;
+    cudaEvent_t t[4] = {nullptr, nullptr, nullptr, nullptr};  // timing: record, reverse sweep
+    // device time of the last record and reverse sweep (ms)
+    double ms_record = 0.0, ms_reverse = 0.0;
 };
 
 }  // namespace ns2d
@@ -106,9 +115,15 @@ bool with_adj_size(int n, F&& f) {
 size_t plane_elems(const ns2d_handle* h) { return (size_t)h->nx * h->ny; }
 
 void free_state(AdjointState* a) {
-    void* ptrs[] = {a->ckpt, a->cap, a->lam[0], a->lam[1], a->w_final, a->dpart};
+    void* ptrs[] = {a->ckpt, a->cap[0], a->cap[1], a->lam[0], a->lam[1], a->P[0], a->P[1],
+                    a->P[2], a->P[3], a->mu, a->w_final, a->dpart};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    cudaEvent_t evs[] = {a->rec_done[0], a->rec_done[1], a->adj_done[0], a->adj_done[1], a->join,
+                         a->t[0], a->t[1], a->t[2], a->t[3]};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    if (a->stream) cudaStreamDestroy(a->stream);
 }
 
 AdjointState* state_of(ns2d_handle* h) {
@@ -129,20 +144,32 @@ ns2d_status ensure_buffers(ns2d_handle* h, int nsteps, int every) {
         ACK(h, cudaMalloc(&a->ckpt, h->field_bytes * nck));
         a->ckpt_n = nck;
     }
-    if (a->cap_steps < seg) {
-        if (a->cap) cudaFree(a->cap);
-        a->cap = nullptr;
-        a->cap_steps = 0;
-        ACK(h, cudaMalloc(&a->cap, h->elem * 8 * plane_elems(h) * seg));
-        a->cap_steps = seg;
-    }
-    for (int k = 0; k < 2; ++k)
-        if (!a->lam[k]) {
-            ACK(h, cudaMalloc(&a->lam[k], h->field_bytes));
-            ACK(h, cudaMemsetAsync(a->lam[k], 0, h->field_bytes, h->stream));
+    // the second capture buffer only when there is more than one segment
+    const int ncap = nck > 1 ? 2 : 1;
+    for (int b = 0; b < ncap; ++b)
+        if (a->cap_steps[b] < seg) {
+            if (a->cap[b]) cudaFree(a->cap[b]);
+            a->cap[b] = nullptr;
+            a->cap_steps[b] = 0;
+            ACK(h, cudaMalloc(&a->cap[b], h->elem * 8 * plane_elems(h) * seg));
+            a->cap_steps[b] = seg;
         }
-    if (!a->w_final) ACK(h, cudaMalloc(&a->w_final, h->field_bytes));
+    void** fields[] = {&a->lam[0], &a->lam[1], &a->P[0], &a->P[1], &a->P[2], &a->P[3], &a->mu, &a->w_final};
+    for (void** f : fields)
+        if (!*f) {
+            ACK(h, cudaMalloc(f, h->field_bytes));
+            ACK(h, cudaMemsetAsync(*f, 0, h->field_bytes, h->stream));
+        }
     if (!a->dpart) ACK(h, cudaMalloc(&a->dpart, sizeof(double) * kRedBlocks));
+    if (!a->stream) {
+        ACK(h, cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            ACK(h, cudaEventCreateWithFlags(&a->rec_done[b], cudaEventDisableTiming));
+            ACK(h, cudaEventCreateWithFlags(&a->adj_done[b], cudaEventDisableTiming));
+        }
+        ACK(h, cudaEventCreateWithFlags(&a->join, cudaEventDisableTiming));
+        for (auto& e : a->t) ACK(h, cudaEventCreate(&e));
+    }
     if (!a->ready) {
         cudaError_t e = cudaSuccess;
         bool ok = h->fp32 ? with_adj_size<float>(h->nx, [&](auto L) { e = decltype(L)::setup(); })
@@ -186,97 +213,119 @@ AdjColArgs<Real> col_common(ns2d_handle* h) {
     return a;
 }
 
-// One adjoint step over the captured stage fields `cap` (8 planes):
-// lam_x = (step Jacobian)^T lam_p.
+// One adjoint step over the captured stage fields `cap` (8 planes), on the
+// adjoint stream: lam_x = (step Jacobian)^T lam_p.
 template <typename Real>
 void adjoint_step(ns2d_handle* h, const void* cap, const void* lam_p, void* lam_x, double dt) {
     using C = typename Cx<Real>::T;
+    AdjointState* st = h->adj;
     AdjColArgs<Real> a = col_common<Real>(h);
+    a.P0 = (const C*)st->P[0];
+    a.P1 = (const C*)st->P[1];
+    a.P2 = (const C*)st->P[2];
+    a.P3 = (const C*)st->P[3];
+    a.mu = (C*)st->mu;
     a.lam_p = (const C*)lam_p;
     a.lam_x = (C*)lam_x;
     AdjRowArgs<Real> r;
     std::memset(&r, 0, sizeof(r));
-    r.mu = (const C*)h->nl;
-    r.P0 = (C*)h->f[0];
-    r.P1 = (C*)h->f[1];
-    r.P2 = (C*)h->f[2];
-    r.P3 = (C*)h->f[3];
+    r.mu = (const C*)st->mu;
+    r.P0 = (C*)st->P[0];
+    r.P1 = (C*)st->P[1];
+    r.P2 = (C*)st->P[2];
+    r.P3 = (C*)st->P[3];
     r.tw = (const C*)h->tw;
     r.ldc = h->ldc;
     const size_t plane = plane_elems(h);
     const C* capc = (const C*)cap;
+    cudaStream_t s = st->stream;
     with_adj_size<Real>(h->nx, [&](auto L) {
         using LL = decltype(L);
         a.b_next = kB[3];
-        LL::col(ADJ_START, a, h->stream);
-        for (int s = 4; s >= 1; --s) {
-            r.cap_uv = capc + (size_t)(2 * (s - 1)) * plane;
+        LL::col(ADJ_START, a, s);
+        for (int stage = 4; stage >= 1; --stage) {
+            r.cap_uv = capc + (size_t)(2 * (stage - 1)) * plane;
             r.cap_w = r.cap_uv + plane;
-            LL::row(r, h->stream);
-            if (s > 1) {
-                a.b_next = kB[s - 2];
-                a.adt = kA[s - 2] * dt;
-                LL::col(ADJ_MID, a, h->stream);
+            LL::row(r, s);
+            if (stage > 1) {
+                a.b_next = kB[stage - 2];
+                a.adt = kA[stage - 2] * dt;
+                LL::col(ADJ_MID, a, s);
             } else {
-                LL::col(ADJ_END, a, h->stream);
+                LL::col(ADJ_END, a, s);
             }
         }
     });
     h->launches += 9;
 }
 
+// Recompute segment `seg` from its checkpoint on the handle's stream, the row
+// passes capturing every stage into capture buffer `buf`.
+ns2d_status recompute_segment(ns2d_handle* h, int seg, int buf) {
+    AdjointState* a = h->adj;
+    const size_t step_bytes = h->elem * 8 * plane_elems(h);
+    const int k0 = seg * a->every;
+    const int k1 = std::min(k0 + a->every, a->nsteps);
+    ACK(h, cudaMemcpyAsync(h->state, (char*)a->ckpt + (size_t)seg * h->field_bytes, h->field_bytes,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    ns2d_status st = NS2D_OK;
+    for (int k = k0; k < k1 && st == NS2D_OK; ++k) {
+        h->cap_step = (char*)a->cap[buf] + (size_t)(k - k0) * step_bytes;
+        st = internal::rk4_step(h, a->dt);
+    }
+    h->cap_step = nullptr;
+    if (st) return st;
+    if (h->cn_dt != a->dt || h->cn_branch != a->branch)
+        return fail(h, NS2D_ERR_STATE, "operator branch changed between record and reverse sweep");
+    ACK(h, cudaEventRecord(a->rec_done[buf], h->stream));
+    return NS2D_OK;
+}
+
 // Reverse sweep over the recorded run: adj->lam[0] holds lambda(T) on entry and
 // lambda(0) on return.  The state is left at the recorded final state.
+// Segment k's adjoint steps (adjoint stream, capture buffer k % 2) overlap the
+// recomputation of segment k-1 (handle stream, buffer (k-1) % 2); each buffer
+// is rewritten only after the adjoint steps that read it are done.
 template <typename Real>
 ns2d_status backward_impl(ns2d_handle* h) {
     AdjointState* a = h->adj;
-    const size_t plane = plane_elems(h);
-    const size_t step_bytes = h->elem * 8 * plane;
+    const size_t step_bytes = h->elem * 8 * plane_elems(h);
     const int nck = (a->nsteps + a->every - 1) / a->every;
     void* lp = a->lam[0];
     void* lx = a->lam[1];
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    for (auto& e : ev) ACK(h, cudaEventCreate(&e));
-    float t_rec = 0.f, t_adj = 0.f;
-    ns2d_status st = NS2D_OK;
+    ACK(h, cudaEventRecord(a->t[2], h->stream));
+    ACK(h, cudaStreamWaitEvent(a->stream, a->t[2], 0));  // lambda(T) is written on the handle's stream
+    ns2d_status st = recompute_segment(h, nck - 1, (nck - 1) & 1);
     for (int seg = nck - 1; seg >= 0 && st == NS2D_OK; --seg) {
+        const int buf = seg & 1;
         const int k0 = seg * a->every;
         const int k1 = std::min(k0 + a->every, a->nsteps);
-        cudaEventRecord(ev[0], h->stream);
-        cudaMemcpyAsync(h->state, (char*)a->ckpt + (size_t)seg * h->field_bytes, h->field_bytes,
-                        cudaMemcpyDeviceToDevice, h->stream);
-        for (int k = k0; k < k1 && st == NS2D_OK; ++k) {
-            h->cap_step = (char*)a->cap + (size_t)(k - k0) * step_bytes;
-            st = internal::rk4_step(h, a->dt);
-        }
-        h->cap_step = nullptr;
-        if (st) break;
-        if (h->cn_dt != a->dt || h->cn_branch != a->branch) {
-            st = fail(h, NS2D_ERR_STATE, "operator branch changed between record and reverse sweep");
-            break;
-        }
-        cudaEventRecord(ev[1], h->stream);
+        ACK(h, cudaStreamWaitEvent(a->stream, a->rec_done[buf], 0));
         for (int k = k1 - 1; k >= k0; --k) {
-            adjoint_step<Real>(h, (const char*)a->cap + (size_t)(k - k0) * step_bytes, lp, lx, a->dt);
+            adjoint_step<Real>(h, (const char*)a->cap[buf] + (size_t)(k - k0) * step_bytes, lp, lx, a->dt);
             std::swap(lp, lx);
         }
-        cudaEventRecord(ev[2], h->stream);
-        cudaEventSynchronize(ev[2]);
-        float m1 = 0.f, m2 = 0.f;
-        cudaEventElapsedTime(&m1, ev[0], ev[1]);
-        cudaEventElapsedTime(&m2, ev[1], ev[2]);
-        t_rec += m1;
-        t_adj += m2;
+        ACK(h, cudaEventRecord(a->adj_done[buf], a->stream));
+        if (seg > 0) {
+            // buffer (seg-1) & 1 was last read by segment seg+1's adjoint steps
+            if (seg + 1 < nck) ACK(h, cudaStreamWaitEvent(h->stream, a->adj_done[(seg + 1) & 1], 0));
+            st = recompute_segment(h, seg - 1, (seg - 1) & 1);
+        }
     }
-    for (auto& e : ev) cudaEventDestroy(e);
+    // join: the handle's stream continues after the last adjoint step
+    ACK(h, cudaEventRecord(a->join, a->stream));
+    ACK(h, cudaStreamWaitEvent(h->stream, a->join, 0));
     if (st) return st;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("adjoint launch: ") + cudaGetErrorString(e));
     if (lp != a->lam[0]) ACK(h, cudaMemcpyAsync(a->lam[0], lp, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
     ACK(h, cudaMemcpyAsync(h->state, a->w_final, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
-    a->ms_recompute = t_rec;
-    a->ms_adjoint = t_adj;
-    return internal::check_status(h);
+    ACK(h, cudaEventRecord(a->t[3], h->stream));
+    ns2d_status s2 = internal::check_status(h);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a->t[2], a->t[3]);
+    a->ms_reverse = ms;
+    return s2;
 }
 
 ns2d_status backward(ns2d_handle* h) {
@@ -310,13 +359,18 @@ ns2d_status record(ns2d_handle* h, int nsteps, double dt, int every) {
     if ((s = ensure_buffers(h, nsteps, every))) return s;
     AdjointState* a = h->adj;
     a->recorded = false;
+    ACK(h, cudaEventRecord(a->t[0], h->stream));
     for (int k = 0; k < nsteps; ++k) {
         if (k % every == 0)
             ACK(h, cudaMemcpyAsync((char*)a->ckpt + (size_t)(k / every) * h->field_bytes, h->state, h->field_bytes,
                                    cudaMemcpyDeviceToDevice, h->stream));
         if ((s = internal::rk4_step(h, dt))) return s;
     }
+    ACK(h, cudaEventRecord(a->t[1], h->stream));
     if ((s = internal::check_status(h))) return s;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a->t[0], a->t[1]);
+    a->ms_record = ms;
     ACK(h, cudaMemcpyAsync(a->w_final, h->state, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
     a->nsteps = nsteps;
     a->every = every;
@@ -401,10 +455,10 @@ ns2d_status ns2d_adjoint_gradient(ns2d_handle* h, int32_t nsteps, double dt, int
     return NS2D_OK;
 }
 
-ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_recompute, double* ms_adjoint) {
+ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_record, double* ms_reverse) {
     if (!h || !h->adj) return NS2D_ERR_INVALID;
-    if (ms_recompute) *ms_recompute = h->adj->ms_recompute;
-    if (ms_adjoint) *ms_adjoint = h->adj->ms_adjoint;
+    if (ms_record) *ms_record = h->adj->ms_record;
+    if (ms_reverse) *ms_reverse = h->adj->ms_reverse;
     return NS2D_OK;
 }
 

@@ -192,6 +192,7 @@ class Solver:
         return v.value, g
 
     def adjoint_times(self):
+        """Device ms of the last adjoint_record and of the last reverse sweep."""
         a, b = C.c_double(), C.c_double()
         self._ck(self.L.ns2d_adjoint_times(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value

@@ -217,6 +217,80 @@ def ensemble_bench(stream, flush, steps, warmup, rank):
     return steps / (ms * 1e-3), ms / steps, grids, launches, z
 
 
+ADJ_N, ADJ_DT, ADJ_EVERY = 512, 5e-4, 50
+
+
+def adjoint_bench(stream, nsteps, rank, precision, g_ref=None, n_dirs=16):
+    """Discrete adjoint at 512^2 (nu = 1e-3, dt = 5e-4, RK4CN, checkpoints every
+    50 steps): device time of one gradient of the final enstrophy (record +
+    objective + checkpointed reverse sweep) over the time of the forward solve
+    alone, from w0 = decaying spectrum (k0 = 4) projected to E = 0.5, Z = 10.
+    FP64: central differences (eps = 1e-6, |d|_W = |w0|_W) of the forward along
+    n_dirs seeded directions.  FP32: the gradient against the FP64 one (g_ref)."""
+    import torch
+    from ns2d import Solver, abi, initial
+    from ns2d import adjoint as nadj
+    p = abi.default_params(nx=ADJ_N, ny=ADJ_N, nu=1e-3, quirks=0, dt=ADJ_DT, precision=precision)
+    s = Solver(p)
+    s.set_stream(stream.cuda_stream)
+    w0 = nadj.project(initial.decaying(ADJ_N, seed=50 + rank, k0=4.0, dealias="2/3"), 0.5, 10.0)
+    c = initial.weights(ADJ_N, ADJ_N)
+
+    def wdot(a, b):
+        return float(np.sum(c * (a.real * b.real + a.imag * b.imag)))
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def forward():
+        s.step_async(nsteps, ADJ_DT)
+
+    def gradient():
+        return s.adjoint_gradient(nsteps, ADJ_DT, ADJ_EVERY, abi.OBJ_ENSTROPHY)
+
+    # warm-up (allocations, kernel set-up), then timed
+    s.set_w_hat(w0)
+    gradient()
+    s.set_w_hat(w0)
+    ms_fwd, _ = timed(forward)
+    s.check()
+    s.set_w_hat(w0)
+    ms_grad, (J, g) = timed(gradient)
+    ms_rec, ms_rev = s.adjoint_times()
+    out = {"precision": "f64" if precision == abi.FP64 else "f32", "forward_ms": ms_fwd, "gradient_ms": ms_grad,
+           "adjoint_over_forward": ms_grad / ms_fwd, "record_ms": ms_rec, "reverse_sweep_ms": ms_rev,
+           "J_final_enstrophy": J}
+    if precision == abi.FP64:
+        rng = np.random.default_rng(900 + rank)
+        rel, scaled = [], []
+        gn = np.sqrt(wdot(g, g))
+        for _ in range(n_dirs):
+            d = initial.dealias_23(initial.hermitian(rng.standard_normal(w0.shape) + 1j * rng.standard_normal(w0.shape)))
+            d *= np.sqrt(wdot(w0, w0) / wdot(d, d))
+            vals = []
+            for sgn in (1.0, -1.0):
+                s.set_w_hat(w0 + sgn * 1e-6 * d)
+                s.step_n(nsteps, ADJ_DT)
+                vals.append(s.objective(abi.OBJ_ENSTROPHY))
+            fd = (vals[0] - vals[1]) / 2e-6
+            ad = wdot(g, d)
+            rel.append(abs(fd - ad) / abs(fd))
+            scaled.append(abs(fd - ad) / (gn * np.sqrt(wdot(d, d))))
+        out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel), "median_rel_err": float(np.median(rel)),
+                     "max_err_over_grad_norm": max(scaled)}
+        out["gradient"] = g
+    elif g_ref is not None:
+        out["grad_rel_err_vs_f64"] = float(np.abs(g - g_ref).max() / np.abs(g_ref).max())
+    s.close()
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -291,6 +365,12 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(te2, op=dist.ReduceOp.MAX)
     ens_total = world * 1e3 / float(te2.item())
 
+    # discrete adjoint at 512^2, FP64 and FP32 (same process, same GPU)
+    from ns2d import abi as _abi
+    adj64 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP64)
+    adj32 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP32, g_ref=adj64.pop("gradient"))
+    adj = [adj64, adj32]
+
     if rank != 0:
         s.close()
         return 0
@@ -326,6 +406,11 @@ def run_gpu(args, rank, world, local_rank):
             "tuned_grids": {"col": ens_grids[0], "row": ens_grids[1]}, "gpu_launches": int(ens_launches),
             "enstrophy_sample": ens_z, "launches_per_step": 9,
         },
+        "adjoint": {
+            "workload": f"gradient of Z(T) w.r.t. w0, {ADJ_N}^2, nu=1e-3, RK4CN dt={ADJ_DT}, {args.adj_steps} steps, "
+                        f"checkpoints every {ADJ_EVERY} steps with stage recomputation",
+            "adjoint_over_forward": adj[0]["adjoint_over_forward"], "runs": adj,
+        },
     }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -348,6 +433,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-steps", type=int, default=20)
+    ap.add_argument("--adj-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -257,8 +257,9 @@ ns2d_status ns2d_objective(ns2d_handle* h, int32_t kind, double* value, double* 
 /* The whole gradient: record, J(w(T)), reverse sweep; grad (host) = dJ/dw(0). */
 ns2d_status ns2d_adjoint_gradient(ns2d_handle* h, int32_t nsteps, double dt, int32_t checkpoint_every,
                                   int32_t kind, double* value, double* grad);
-/* Device time (ms) of the last reverse sweep: stage recomputation, adjoint steps. */
-ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_recompute, double* ms_adjoint);
+/* Device time (ms) of the last ns2d_adjoint_record and of the last reverse
+   sweep (stage recomputation and adjoint steps, which overlap on two streams). */
+ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_record, double* ms_reverse);
 /* <a, b>_W of two device arrays, accumulated in FP64. */
 ns2d_status ns2d_wdot_device(ns2d_handle* h, const double* d_a, const double* d_b, double* value);
 
