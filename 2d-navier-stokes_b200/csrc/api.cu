@@ -87,8 +87,6 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.norm2 = (Real)std::pow(norm_fac, 2.0);
     a.inv_nxny = norm_fac;
     a.status = h->dstatus;
-    a.blowup_sum = h->dscal;
-    a.partials = h->dpart;
     a.final_tail = 1;
     a.ntiles = (h->nyf + col_tc(h->nx) - 1) / col_tc(h->nx);
     a.lin = make_lin(h, branch);
@@ -464,6 +462,57 @@ ns2d_status unpack_out(ns2d_handle* h, const void* src, double2* d_dst) {
 
 #define DISPATCH(h, fn, ...) ((h)->fp32 ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
 
+void drop_graph(ns2d_handle* h) {
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+    h->graph_branch = -1;
+}
+
+// One fixed-dt RK4/RK4CN step for the time loops (ns2d_step_n, ns2d_step_async).
+// The first step with a given dt runs eagerly (it settles the operator branch
+// and the CN table); the step is then captured once as a CUDA graph of its
+// nine launches and replayed for the following steps.  Kernel timing and
+// adjoint capture use the eager form.
+ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
+    if (h->timing || h->cap_step) return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    int hf = h->hyper_flag;
+    const int branch = (h->p.system == NS2D_EULER && h->p.integrator != NS2D_RK4)
+                           ? 4
+                           : ns2d::resolve_branch(hf, h->p.ekmn_drag_flag, quirk(h, NS2D_QUIRK_HYPER_LATCH));
+    const bool settled = (hf == h->hyper_flag) && h->cn_dt == dt && h->cn_branch == branch;
+    if (h->step_graph && h->graph_dt == dt && h->graph_branch == branch && settled) {
+        cudaError_t e = cudaGraphLaunch(h->step_graph, h->stream);
+        if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+        h->launches += 9;
+        return NS2D_OK;
+    }
+    drop_graph(h);
+    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    if (s) return s;
+    // capture the next steps' launches (recorded, not executed)
+    const int64_t l0 = h->launches;
+    cudaGraph_t g = nullptr;
+    CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = l0;
+    if (s) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->step_graph = nullptr;
+        return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    h->graph_dt = dt;
+    h->graph_branch = h->cn_branch;
+    return NS2D_OK;
+}
+
+
 ns2d_status host_to_state(ns2d_handle* h, const double* host, void* dst) {
     CK(h, cudaMemcpyAsync(h->dio, host, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyHostToDevice, h->stream));
     return DISPATCH(h, pack_in, h, h->dio, dst);
@@ -684,6 +733,7 @@ ns2d_status ns2d_destroy(ns2d_handle* h) {
     if (!h) return NS2D_ERR_INVALID;
     cudaSetDevice(h->p.device);
     cudaStreamSynchronize(h->stream);
+    drop_graph(h);
     internal::adjoint_free(h);
     free_all(h);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
@@ -812,7 +862,7 @@ ns2d_status ns2d_step_n(ns2d_handle* h, int32_t nsteps, double dt) {
             } else if (h->p.integrator == NS2D_AB4) {
                 s = DISPATCH(h, ab4_update_impl, h, dt);
             } else {
-                s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+                s = rk4_step_loop(h, dt);
             }
             if (s) return s;
         }
@@ -986,7 +1036,7 @@ ns2d_status ns2d_step_async(ns2d_handle* h, int32_t nsteps, double dt) {
         } else if (h->p.integrator == NS2D_AB4) {
             s = DISPATCH(h, ab4_update_impl, h, dt);
         } else {
-            s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+            s = rk4_step_loop(h, dt);
         }
         if (s) return s;
     }

@@ -63,6 +63,10 @@ struct ns2d_handle {
     // adjoint's own buffers (adjoint.cu)
     void* cap_step = nullptr;
     ns2d::AdjointState* adj = nullptr;
+    // one RK4/RK4CN step captured as a CUDA graph for fixed-dt stepping
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    int graph_branch = -1;
 };
 
 namespace ns2d {

@@ -100,8 +100,6 @@ struct ColArgs {
     int lin_stage;       // 0 none, 1: rhs += dt D X (quirk), 2: rhs -= D X (corrected)
     LinOp lin;
     const double2* cn;   // COL_FINAL, CN schemes: per-mode ((2-D)/(2+D), 2dt/(2+D)), stride ldc
-    double* blowup_sum;  // COL_FINAL: [1] holds the ticket counter
-    double* partials;    // COL_FINAL: one partial bound per block
     double inv_nxny;     // 1/(Nx Ny)
     int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
     int ntiles;          // number of column tiles of this field
@@ -166,20 +164,38 @@ struct ColSmem {
     static constexpr size_t bytes() { return sizeof(C) * (size_t)(2 * FFT + PRE); }
 };
 
-// Derived spectrum f of the stage input X at (kx, ky) (solver.c:904-957):
-// 0: i ky/k^2 X, 1: -i kx/k^2 X, 2: i kx X, 3: i ky X.
+// 1/k^2 for the velocity spectra: the correctly rounded reciprocal (the same
+// value as 1.0/k2) in FP64, single precision in the FP32 form.
+template <typename Real>
+__device__ __forceinline__ Real inv_k2(int k2);
+template <>
+__device__ __forceinline__ double inv_k2<double>(int k2) { return __drcp_rn((double)k2); }
+template <>
+__device__ __forceinline__ float inv_k2<float>(int k2) { return __frcp_rn((float)k2); }
+
+// Derived spectra of the stage input X at (kx, ky) (solver.c:904-957), two at a
+// time: pair 0 gives u = i ky/k^2 X and v = -i kx/k^2 X (one reciprocal), pair 2
+// gives w_x = i kx X and w_y = i ky X.  Zero at the mean mode.
 template <typename C>
-__device__ __forceinline__ C derived(int f, int kx, int ky, C X) {
+__device__ __forceinline__ void derived_pair(int fp, int kx, int ky, C X, C& a, C& b) {
     using Real = decltype(C::x);
-    if (kx == 0 && ky == 0) return cmake<C>(0, 0);
-    Real s;
-    if (f < 2) {
-        const double inv = 1.0 / (double)(kx * kx + ky * ky);
-        s = (Real)((double)(f == 0 ? ky : kx) * inv);
-    } else {
-        s = (Real)(f == 2 ? kx : ky);
+    if (kx == 0 && ky == 0) {
+        a = cmake<C>(0, 0);
+        b = a;
+        return;
     }
-    return (f == 1) ? cmake<C>(s * X.y, -s * X.x) : cmake<C>(-s * X.y, s * X.x);
+    Real sa, sb;
+    if (fp == 0) {
+        const Real inv = inv_k2<Real>(kx * kx + ky * ky);
+        sa = (Real)ky * inv;
+        sb = -(Real)kx * inv;
+    } else {
+        sa = (Real)kx;
+        sb = (Real)ky;
+    }
+    // i s X = (-s X.y, s X.x)
+    a = cmake<C>(-sa * X.y, sa * X.x);
+    b = cmake<C>(-sb * X.y, sb * X.x);
 }
 
 // Column pass on tile `tile` (ky columns tile*TC .. tile*TC+TC-1), by the T*TC
@@ -349,14 +365,14 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             }
             // SystemCheck (solver.c:2301-2326) without a transform: max|w(x)| is
             // bounded by sum|w_hat|/(Nx Ny) over the full spectrum.  Status bit 1:
-            // non-finite state; bit 2: bound >= 1e100 (the host then evaluates
-            // max|w| exactly).  Each block writes its partial sum; the last block
-            // to finish (atomic ticket, no waiting) adds them up.
+            // non-finite state; bit 2: the bound may reach 1e100 (the host then
+            // evaluates max|w| exactly).  A bound of 1e100 needs one tile whose
+            // share is at least 1e100/ntiles, so each block tests its own share
+            // and no cross-block reduction is needed.
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
             const unsigned anybad = __ballot_sync(0xffffffffu, bad);
             double* wsum = reinterpret_cast<double*>(smraw);  // parked slots are free again
-            __shared__ int is_last;
             const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
             const int nwarps = (int)(blockDim.x >> 5);
             if (lane == 0) {
@@ -364,32 +380,13 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 if (anybad) atomicOr(a.status, 1);
             }
             __syncthreads();
-            unsigned int* ticket = reinterpret_cast<unsigned int*>(a.blowup_sum + 1);
             if (threadIdx.x == 0) {
                 double tot = 0.0;
                 for (int w = 0; w < nwarps; ++w) tot += wsum[w];
-                a.partials[tile] = tot;
-                __threadfence();
-                is_last = (atomicAdd(ticket, 1u) == (unsigned int)a.ntiles - 1);
+                if (!(tot * a.inv_nxny < 1e100 / (double)a.ntiles)) atomicOr(a.status, 2);
+                if (tile == 0) atomicAdd(a.status + 1, 1);  // completed steps
             }
             __syncthreads();
-            if (is_last) {
-                __threadfence();
-                double v = 0.0;
-                for (int b = threadIdx.x; b < a.ntiles; b += blockDim.x) v += __ldcg(a.partials + b);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) wsum[nwarps + warp] = v;
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    double total = 0.0;
-                    for (int w = 0; w < nwarps; ++w) total += wsum[nwarps + w];
-                    if (!(total * a.inv_nxny < 1e100)) atomicOr(a.status, 2);
-                    *ticket = 0u;
-                    atomicAdd(a.status + 1, 1);  // completed steps
-                    __threadfence();
-                }
-            }
             return;
         }
         if constexpr (MODE == COL_RHS) return;
@@ -405,9 +402,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
             const int kx = (i <= N / 2) ? i : i - N;
-            const C X = pre0[i * TC + c];
-            v[0][m] = derived(fp, kx, ky, X);
-            v[1][m] = derived(fp + 1, kx, ky, X);
+            derived_pair(fp, kx, ky, pre0[i * TC + c], v[0][m], v[1][m]);
         }
         fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
         if (valid) {

@@ -316,7 +316,6 @@ def run_gpu(args, rank, world, local_rank):
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize(dev)
-    s.set_kernel_timing(True)
     l0 = s.launch_count
     with ClockSampler(local_rank) as clk:
         with torch.cuda.stream(stream):
@@ -330,6 +329,15 @@ def run_gpu(args, rank, world, local_rank):
     launches = s.launch_count - l0
     barrier()
     ms_total = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    # per-kernel device times (events around every launch; eager launches, so
+    # this loop is separate from the timed steps above, which replay a graph)
+    s.set_kernel_timing(True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            s.step_async(1, DT)
+            flush.zero_()
+    torch.cuda.synchronize(dev)
+    s.check()
     kms, kn = s.kernel_times()
     s.set_kernel_timing(False)
     t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
