@@ -59,6 +59,13 @@ struct AdjointState {
     cudaEvent_t t[4] = {nullptr, nullptr, nullptr, nullptr};  // timing: record, reverse sweep
     // device time of the last record and reverse sweep (ms)
     double ms_record = 0.0, ms_reverse = 0.0;
+    // full-length segments replay captured graphs: the recomputation into
+    // capture buffer b, and the adjoint steps over buffer b starting from
+    // lambda buffer p
+    cudaGraphExec_t rec_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t adj_graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_every = 0, graph_branch = -1;
+    double graph_dt = 0.0;
 };
 
 }  // namespace ns2d
@@ -114,7 +121,22 @@ bool with_adj_size(int n, F&& f) {
 
 size_t plane_elems(const ns2d_handle* h) { return (size_t)h->nx * h->ny; }
 
+void drop_graphs(AdjointState* a) {
+    for (auto& g : a->rec_graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    for (auto& row : a->adj_graph)
+        for (auto& g : row) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    a->graph_every = 0;
+    a->graph_branch = -1;
+}
+
 void free_state(AdjointState* a) {
+    drop_graphs(a);
     void* ptrs[] = {a->ckpt, a->cap[0], a->cap[1], a->lam[0], a->lam[1], a->P[0], a->P[1],
                     a->P[2], a->P[3], a->mu, a->w_final, a->dpart};
     for (void* p : ptrs)
@@ -148,6 +170,7 @@ ns2d_status ensure_buffers(ns2d_handle* h, int nsteps, int every) {
     const int ncap = nck > 1 ? 2 : 1;
     for (int b = 0; b < ncap; ++b)
         if (a->cap_steps[b] < seg) {
+            drop_graphs(a);
             if (a->cap[b]) cudaFree(a->cap[b]);
             a->cap[b] = nullptr;
             a->cap_steps[b] = 0;
@@ -259,25 +282,103 @@ void adjoint_step(ns2d_handle* h, const void* cap, const void* lam_p, void* lam_
     h->launches += 9;
 }
 
-// Recompute segment `seg` from its checkpoint on the handle's stream, the row
-// passes capturing every stage into capture buffer `buf`.
-ns2d_status recompute_segment(ns2d_handle* h, int seg, int buf) {
+// Ends a stream capture and instantiates it.
+ns2d_status end_capture(ns2d_handle* h, cudaStream_t st, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    return NS2D_OK;
+}
+
+// The steps k0..k1-1 of the recorded run from the state, the row passes
+// capturing every stage into capture buffer `buf` (eager launches).
+ns2d_status recompute_steps(ns2d_handle* h, int k0, int k1, int buf) {
     AdjointState* a = h->adj;
     const size_t step_bytes = h->elem * 8 * plane_elems(h);
-    const int k0 = seg * a->every;
-    const int k1 = std::min(k0 + a->every, a->nsteps);
-    ACK(h, cudaMemcpyAsync(h->state, (char*)a->ckpt + (size_t)seg * h->field_bytes, h->field_bytes,
-                           cudaMemcpyDeviceToDevice, h->stream));
     ns2d_status st = NS2D_OK;
     for (int k = k0; k < k1 && st == NS2D_OK; ++k) {
         h->cap_step = (char*)a->cap[buf] + (size_t)(k - k0) * step_bytes;
         st = internal::rk4_step(h, a->dt);
     }
     h->cap_step = nullptr;
+    return st;
+}
+
+// Recompute segment `seg` from its checkpoint on the handle's stream into
+// capture buffer `buf`; full-length segments replay a captured graph.
+ns2d_status recompute_segment(ns2d_handle* h, int seg, int buf) {
+    AdjointState* a = h->adj;
+    const int k0 = seg * a->every;
+    const int k1 = std::min(k0 + a->every, a->nsteps);
+    ACK(h, cudaMemcpyAsync(h->state, (char*)a->ckpt + (size_t)seg * h->field_bytes, h->field_bytes,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    ns2d_status st = NS2D_OK;
+    if (k1 - k0 == a->every && a->every > 1) {
+        if (!a->rec_graph[buf]) {
+            const int64_t l0 = h->launches;
+            const bool timing = h->timing;  // no per-launch events inside the graph
+            h->timing = false;
+            ACK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            st = recompute_steps(h, k0, k1, buf);
+            cudaGraphExec_t g = nullptr;
+            ns2d_status st2 = end_capture(h, h->stream, &g);
+            h->timing = timing;
+            h->launches = l0;
+            if (st) {
+                if (g) cudaGraphExecDestroy(g);
+                return st;
+            }
+            if (st2) return st2;
+            a->rec_graph[buf] = g;
+        }
+        ACK(h, cudaGraphLaunch(a->rec_graph[buf], h->stream));
+        h->launches += 9 * (k1 - k0);
+    } else {
+        st = recompute_steps(h, k0, k1, buf);
+    }
     if (st) return st;
     if (h->cn_dt != a->dt || h->cn_branch != a->branch)
         return fail(h, NS2D_ERR_STATE, "operator branch changed between record and reverse sweep");
     ACK(h, cudaEventRecord(a->rec_done[buf], h->stream));
+    return NS2D_OK;
+}
+
+// The adjoint steps of a segment of n steps over capture buffer `buf`, on the
+// adjoint stream, starting from lambda buffer `par`; returns the parity after.
+template <typename Real>
+void adjoint_steps(ns2d_handle* h, int n, int buf, int par) {
+    AdjointState* a = h->adj;
+    const size_t step_bytes = h->elem * 8 * plane_elems(h);
+    for (int k = n - 1; k >= 0; --k) {
+        adjoint_step<Real>(h, (const char*)a->cap[buf] + (size_t)k * step_bytes, a->lam[par], a->lam[par ^ 1], a->dt);
+        par ^= 1;
+    }
+}
+
+template <typename Real>
+ns2d_status adjoint_segment(ns2d_handle* h, int n, int buf, int par) {
+    AdjointState* a = h->adj;
+    if (n == a->every && a->every > 1) {
+        cudaGraphExec_t& g = a->adj_graph[buf][par];
+        if (!g) {
+            const int64_t l0 = h->launches;
+            ACK(h, cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal));
+            adjoint_steps<Real>(h, n, buf, par);
+            ns2d_status st = end_capture(h, a->stream, &g);
+            h->launches = l0;
+            if (st) return st;
+        }
+        ACK(h, cudaGraphLaunch(g, a->stream));
+        h->launches += 9 * n;
+    } else {
+        adjoint_steps<Real>(h, n, buf, par);
+    }
     return NS2D_OK;
 }
 
@@ -289,22 +390,27 @@ ns2d_status recompute_segment(ns2d_handle* h, int seg, int buf) {
 template <typename Real>
 ns2d_status backward_impl(ns2d_handle* h) {
     AdjointState* a = h->adj;
-    const size_t step_bytes = h->elem * 8 * plane_elems(h);
     const int nck = (a->nsteps + a->every - 1) / a->every;
-    void* lp = a->lam[0];
-    void* lx = a->lam[1];
+    if (a->graph_every != a->every || a->graph_dt != a->dt || a->graph_branch != a->branch) {
+        drop_graphs(a);
+        a->graph_every = a->every;
+        a->graph_dt = a->dt;
+        a->graph_branch = a->branch;
+    }
+    int par = 0;  // lambda' lives in lam[par]
+    // the CN table of the recorded dt, before any launch reads it
+    ns2d_status s0 = internal::ensure_cn(h, a->dt, a->branch);
+    if (s0) return s0;
     ACK(h, cudaEventRecord(a->t[2], h->stream));
     ACK(h, cudaStreamWaitEvent(a->stream, a->t[2], 0));  // lambda(T) is written on the handle's stream
     ns2d_status st = recompute_segment(h, nck - 1, (nck - 1) & 1);
     for (int seg = nck - 1; seg >= 0 && st == NS2D_OK; --seg) {
         const int buf = seg & 1;
         const int k0 = seg * a->every;
-        const int k1 = std::min(k0 + a->every, a->nsteps);
+        const int n = std::min(k0 + a->every, a->nsteps) - k0;
         ACK(h, cudaStreamWaitEvent(a->stream, a->rec_done[buf], 0));
-        for (int k = k1 - 1; k >= k0; --k) {
-            adjoint_step<Real>(h, (const char*)a->cap[buf] + (size_t)(k - k0) * step_bytes, lp, lx, a->dt);
-            std::swap(lp, lx);
-        }
+        if ((st = adjoint_segment<Real>(h, n, buf, par))) break;
+        par ^= (n & 1);
         ACK(h, cudaEventRecord(a->adj_done[buf], a->stream));
         if (seg > 0) {
             // buffer (seg-1) & 1 was last read by segment seg+1's adjoint steps
@@ -318,7 +424,7 @@ ns2d_status backward_impl(ns2d_handle* h) {
     if (st) return st;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("adjoint launch: ") + cudaGetErrorString(e));
-    if (lp != a->lam[0]) ACK(h, cudaMemcpyAsync(a->lam[0], lp, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    if (par != 0) ACK(h, cudaMemcpyAsync(a->lam[0], a->lam[1], h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
     ACK(h, cudaMemcpyAsync(h->state, a->w_final, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
     ACK(h, cudaEventRecord(a->t[3], h->stream));
     ns2d_status s2 = internal::check_status(h);
@@ -364,7 +470,7 @@ ns2d_status record(ns2d_handle* h, int nsteps, double dt, int every) {
         if (k % every == 0)
             ACK(h, cudaMemcpyAsync((char*)a->ckpt + (size_t)(k / every) * h->field_bytes, h->state, h->field_bytes,
                                    cudaMemcpyDeviceToDevice, h->stream));
-        if ((s = internal::rk4_step(h, dt))) return s;
+        if ((s = internal::rk4_step_loop(h, dt))) return s;
     }
     ACK(h, cudaEventRecord(a->t[1], h->stream));
     if ((s = internal::check_status(h))) return s;

@@ -124,17 +124,33 @@ struct TimedLaunch {
     ns2d_handle* h;
     int cls;
     cudaEvent_t a = nullptr, b = nullptr;
+    bool graph_slot = false;
     TimedLaunch(ns2d_handle* h_, int cls_) : h(h_), cls(cls_) {
-        if (h->timing) {
+        if (!h->timing) return;
+        if (h->capturing_timed && h->gev_n < 16) {
+            // event pair owned by the timed step graph, read after every replay
+            const int k = h->gev_n++;
+            for (int j = 0; j < 2; ++j)
+                if (!h->gev[k][j]) cudaEventCreate(&h->gev[k][j]);
+            a = h->gev[k][0];
+            b = h->gev[k][1];
+            h->gev_cls[k] = cls;
+            graph_slot = true;
+        } else {
             a = take_event(h);
             b = take_event(h);
-            cudaEventRecord(a, h->stream);
         }
+        record(a);
+    }
+    // inside a capture the records become event nodes of the graph
+    void record(cudaEvent_t e) {
+        if (graph_slot) cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
+        else cudaEventRecord(e, h->stream);
     }
     ~TimedLaunch() {
         if (h->timing) {
-            cudaEventRecord(b, h->stream);
-            h->ev_open.push_back({cls, {a, b}});
+            record(b);
+            if (!graph_slot) h->ev_open.push_back({cls, {a, b}});
         }
         h->launches++;
     }
@@ -466,34 +482,17 @@ void drop_graph(ns2d_handle* h) {
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
     h->graph_branch = -1;
+    if (h->timed_graph) cudaGraphExecDestroy(h->timed_graph);
+    h->timed_graph = nullptr;
+    h->timed_branch = -1;
 }
 
-// One fixed-dt RK4/RK4CN step for the time loops (ns2d_step_n, ns2d_step_async).
-// The first step with a given dt runs eagerly (it settles the operator branch
-// and the CN table); the step is then captured once as a CUDA graph of its
-// nine launches and replayed for the following steps.  Kernel timing and
-// adjoint capture use the eager form.
-ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
-    if (h->timing || h->cap_step) return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
-    int hf = h->hyper_flag;
-    const int branch = (h->p.system == NS2D_EULER && h->p.integrator != NS2D_RK4)
-                           ? 4
-                           : ns2d::resolve_branch(hf, h->p.ekmn_drag_flag, quirk(h, NS2D_QUIRK_HYPER_LATCH));
-    const bool settled = (hf == h->hyper_flag) && h->cn_dt == dt && h->cn_branch == branch;
-    if (h->step_graph && h->graph_dt == dt && h->graph_branch == branch && settled) {
-        cudaError_t e = cudaGraphLaunch(h->step_graph, h->stream);
-        if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
-        h->launches += 9;
-        return NS2D_OK;
-    }
-    drop_graph(h);
-    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
-    if (s) return s;
-    // capture the next steps' launches (recorded, not executed)
+// Captures the launches of one RK4/RK4CN step (recorded, not executed).
+ns2d_status capture_step(ns2d_handle* h, double dt, cudaGraphExec_t* out) {
     const int64_t l0 = h->launches;
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = l0;
     if (s) {
@@ -501,17 +500,60 @@ ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
         return s;
     }
     if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-        h->step_graph = nullptr;
+        *out = nullptr;
         return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
     }
-    h->graph_dt = dt;
-    h->graph_branch = h->cn_branch;
     return NS2D_OK;
 }
 
+// One fixed-dt RK4/RK4CN step for the time loops (ns2d_step_n, ns2d_step_async,
+// the adjoint's record).  The first step with a given dt runs eagerly (it
+// settles the operator branch and the CN table); the step is then captured once
+// as a CUDA graph of its nine launches and replayed for the following steps.
+// With kernel timing on, a second graph carries an event pair around every
+// launch and is read back after each replay.  Stage capture for the adjoint
+// uses the eager form.
+ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
+    if (h->cap_step) return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    int hf = h->hyper_flag;
+    const int branch = (h->p.system == NS2D_EULER && h->p.integrator != NS2D_RK4)
+                           ? 4
+                           : ns2d::resolve_branch(hf, h->p.ekmn_drag_flag, quirk(h, NS2D_QUIRK_HYPER_LATCH));
+    const bool settled = (hf == h->hyper_flag) && h->cn_dt == dt && h->cn_branch == branch;
+    cudaGraphExec_t* gx = h->timing ? &h->timed_graph : &h->step_graph;
+    double* gdt = h->timing ? &h->timed_dt : &h->graph_dt;
+    int* gbr = h->timing ? &h->timed_branch : &h->graph_branch;
+    if (!(*gx && *gdt == dt && *gbr == branch && settled)) {
+        if (*gx) cudaGraphExecDestroy(*gx);
+        *gx = nullptr;
+        ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);  // this call's step
+        if (s) return s;
+        h->capturing_timed = h->timing;
+        h->gev_n = 0;
+        s = capture_step(h, dt, gx);
+        h->capturing_timed = false;
+        if (s) return s;
+        *gdt = dt;
+        *gbr = h->cn_branch;
+        return NS2D_OK;
+    }
+    cudaError_t e = cudaGraphLaunch(*gx, h->stream);
+    if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+    h->launches += 9;
+    if (h->timing) {
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (int k = 0; k < h->gev_n; ++k) {
+            float ms = 0.f;
+            CK(h, cudaEventElapsedTime(&ms, h->gev[k][0], h->gev[k][1]));
+            h->t_ms[h->gev_cls[k]] += ms;
+            h->t_n[h->gev_cls[k]] += 1;
+        }
+    }
+    return NS2D_OK;
+}
 
 ns2d_status host_to_state(ns2d_handle* h, const double* host, void* dst) {
     CK(h, cudaMemcpyAsync(h->dio, host, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyHostToDevice, h->stream));
@@ -631,6 +673,8 @@ namespace internal {
 
 ns2d_status fail(ns2d_handle* h, ns2d_status s, const std::string& msg) { return ::fail(h, s, msg); }
 ns2d_status rk4_step(ns2d_handle* h, double dt) { return DISPATCH(h, rk4_step_impl, h, dt, nullptr); }
+ns2d_status rk4_step_loop(ns2d_handle* h, double dt) { return ::rk4_step_loop(h, dt); }
+ns2d_status ensure_cn(ns2d_handle* h, double dt, int branch) { return ::ensure_cn(h, dt, branch); }
 ns2d_status check_status(ns2d_handle* h) { return ::check_status(h); }
 ns2d_status pack_in(ns2d_handle* h, const double2* d_src, void* dst) { return DISPATCH(h, ::pack_in, h, d_src, dst); }
 ns2d_status unpack_out(ns2d_handle* h, const void* src, double2* d_dst) {
@@ -734,6 +778,9 @@ ns2d_status ns2d_destroy(ns2d_handle* h) {
     cudaSetDevice(h->p.device);
     cudaStreamSynchronize(h->stream);
     drop_graph(h);
+    for (auto& pair : h->gev)
+        for (cudaEvent_t e : pair)
+            if (e) cudaEventDestroy(e);
     internal::adjoint_free(h);
     free_all(h);
     for (auto e : h->ev_pool) cudaEventDestroy(e);

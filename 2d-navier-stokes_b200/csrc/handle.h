@@ -67,6 +67,14 @@ struct ns2d_handle {
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
     int graph_branch = -1;
+    // the same with an event pair around every launch (kernel timing mode)
+    cudaGraphExec_t timed_graph = nullptr;
+    double timed_dt = 0.0;
+    int timed_branch = -1;
+    bool capturing_timed = false;
+    int gev_n = 0;
+    cudaEvent_t gev[16][2] = {};
+    int gev_cls[16] = {};
 };
 
 namespace ns2d {
@@ -75,6 +83,10 @@ namespace internal {
 ns2d_status fail(ns2d_handle* h, ns2d_status s, const std::string& msg);
 // One RK4 / RK4CN step in the handle's precision (no status read-back).
 ns2d_status rk4_step(ns2d_handle* h, double dt);
+// The same through the fixed-dt graph replay of the time loops.
+ns2d_status rk4_step_loop(ns2d_handle* h, double dt);
+// Crank-Nicolson factor table for (dt, operator branch).
+ns2d_status ensure_cn(ns2d_handle* h, double dt, int branch);
 // Status read-back and SystemCheck after a batch of steps.
 ns2d_status check_status(ns2d_handle* h);
 // complex128 [nx][nyf] device array <-> internal [nx][ldc] field.
