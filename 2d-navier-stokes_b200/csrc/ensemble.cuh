@@ -18,7 +18,7 @@ struct EnsShape {
     static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= 64");
 };
 
-#define NS2D_ENS_SIZES(X) X(64) X(128) X(256) X(512) X(1024)
+#define NS2D_ENS_SIZES(X) X(64) X(128) X(256) X(512)
 
 template <typename Real>
 struct EnsMember {
@@ -69,8 +69,16 @@ __device__ __forceinline__ void ens_apply_stage(ColArgs<Real>& a, const EnsMembe
     }
 }
 
+// Resident 128-thread blocks per SM the ensemble kernels are compiled for: four
+// in FP32 (at most 128 registers a thread), the register need of one FP64
+// body otherwise.
+template <typename Real>
+struct EnsMinBlocks {
+    static constexpr int value = sizeof(Real) == 4 ? 4 : 1;
+};
+
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(128) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
+__global__ void __launch_bounds__(128, EnsMinBlocks<Real>::value) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, EnsStage st) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(st.status)) return;
@@ -92,7 +100,7 @@ __global__ void __launch_bounds__(128) ens_col_kernel(const EnsMember<Real>* __r
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(128) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
+__global__ void __launch_bounds__(128, EnsMinBlocks<Real>::value) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, int* status) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(status)) return;

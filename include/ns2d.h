@@ -264,7 +264,7 @@ ns2d_status ns2d_adjoint_times(const ns2d_handle* h, double* ms_record, double* 
 ns2d_status ns2d_wdot_device(ns2d_handle* h, const double* d_a, const double* d_b, double* value);
 
 /* ---- Batched ensembles -----------------------------------------------------
-   Independent trajectories of possibly different square grid sizes (64..1024)
+   Independent trajectories of possibly different square grid sizes (64..512)
    advanced together: every pass of a step is one launch for all members, and
    the step is replayed from a captured CUDA graph.  The reference has no
    counterpart inside the solver; it runs parameter sweeps as separate
