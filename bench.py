@@ -282,13 +282,34 @@ def adjoint_bench(stream, nsteps, rank, precision, g_ref=None, n_dirs=16):
             ad = wdot(g, d)
             rel.append(abs(fd - ad) / abs(fd))
             scaled.append(abs(fd - ad) / (gn * np.sqrt(wdot(d, d))))
-        out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel), "median_rel_err": float(np.median(rel)),
-                     "max_err_over_grad_norm": max(scaled)}
+        if n_dirs:
+            out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel),
+                         "median_rel_err": float(np.median(rel)), "max_err_over_grad_norm": max(scaled)}
         out["gradient"] = g
     elif g_ref is not None:
         out["grad_rel_err_vs_f64"] = float(np.abs(g - g_ref).max() / np.abs(g_ref).max())
     s.close()
     return out
+
+
+def run_part(args, local_rank):
+    """One part of the benchmark alone (--only): its JSON object on one line.
+    Used for profiling runs, which should hold few launches."""
+    import torch
+    from ns2d import abi
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    if args.only == "ensemble":
+        v, ms, grids, launches, z = ensemble_bench(stream, flush, args.ens_steps, args.warmup, 0)
+        out = {"part": "ensemble", "ensemble_steps_per_s": v, "ms_per_step": ms, "tuned_grids": grids,
+               "gpu_launches": launches, "enstrophy_sample": z}
+    else:
+        out = {"part": "adjoint", "run": adjoint_bench(stream, args.adj_steps, 0, abi.FP64, n_dirs=0)}
+        out["run"].pop("gradient", None)
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -442,6 +463,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--only", choices=["ensemble", "adjoint"], default=None,
+                    help="run one part alone and print its JSON object (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -450,6 +473,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.only:
+        return run_part(args, local_rank)
     if world > 1:
         import datetime
         import torch
