@@ -6,7 +6,11 @@ Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this.
                    (oracle/ns2d_oracle.c), same layouts as include/ns2d.h.
 * ``RefSolver`` -- oracle/_ref/libns2d_ref_<variant>.so, the reference's own
                    Solver/src/{solver,force,sys_msr}.c built by oracle/Makefile
-                   against the single-rank stand-ins in oracle/shim/.
+                   against the single-rank stand-ins in oracle/shim/.  Variant
+                   "dropin" is the same program with its per-step entry points
+                   resolved to the GPU (2d-navier-stokes_b200/compat).
+* ``solve``     -- the reference's own time loop (SpectralSolve) in one of
+                   those libraries; once per process.
 """
 import ctypes as C
 import os
@@ -279,3 +283,31 @@ class RefSolver:
         sp = np.zeros(8 * self.n_spect)
         self.L.ref_system_measurables(t, it, _ptr(s), _ptr(sp))
         return s, sp.reshape(8, self.n_spect)
+
+
+def solve(params, variant="rk4cn", u0="TG_VORT", T=0.05, save_every=10, threads=1):
+    """Run SpectralSolve (Solver/src/solver.c:54-251) of a reference library
+    from the initial condition u0 over [0, T]; returns (w_hat at the last save,
+    its time, number of saves).  The library keeps global state: call once per
+    process (the tests use spawned processes)."""
+    path = _REF_SO.format(variant)
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    L = C.CDLL(path)
+    L.ref_solve.argtypes = [C.c_void_p, C.c_int]
+    L.ref_saved_w_hat.argtypes = [_dp, _dp]
+    L.ref_saved_w_hat.restype = C.c_long
+    forcing = {0: b"NONE", 1: b"KOLM", 2: b"ZERO"}[params.forcing]
+    rp = _RefParams(nx=params.nx, ny=params.ny, nu=params.nu, hyper_visc_flag=params.hyper_visc_flag,
+                    hyper_visc_pow=params.hyper_visc_pow, ekmn_alpha=params.ekmn_alpha,
+                    ekmn_drag_flag=params.ekmn_drag_flag, ekmn_drag_pow=params.ekmn_drag_pow,
+                    force_k=params.force_k, force_scale=params.force_scale, dt=params.dt, t0=0.0,
+                    T=T, adapt_step_flag=params.adapt_step_flag, cfl_cond_flag=params.cfl_cond_flag,
+                    cfl_const=params.cfl_const, save_every=save_every, num_print_steps=4,
+                    forcing=forcing, u0=u0.encode())
+    if L.ref_solve(C.byref(rp), threads) != 0:
+        raise RuntimeError("ref_solve failed")
+    w = np.zeros((params.nx, params.ny // 2 + 1), np.complex128)
+    t = C.c_double()
+    n = L.ref_saved_w_hat(_ptr(w.view(np.float64)), C.byref(t))
+    return w, t.value, int(n)

@@ -67,8 +67,8 @@ int ref_variant(void) {
 #endif
 }
 
-int ref_init(const ref_params* p, int run_initial_conditions, int threads) {
-    if (g_ready) return -1;
+/* main.c:33-60 and GetCMLArgs: globals and parameters, no allocation. */
+static void set_globals(const ref_params* p, int threads) {
     offt_set_threads(threads);
     memset(&g_run, 0, sizeof g_run);
     memset(&g_sys, 0, sizeof g_sys);
@@ -103,6 +103,11 @@ int ref_init(const ref_params* p, int run_initial_conditions, int threads) {
     strncpy(sys_vars->u0, p->u0, 63);
     g_N[0] = p->nx;
     g_N[1] = p->ny;
+}
+
+int ref_init(const ref_params* p, int run_initial_conditions, int threads) {
+    if (g_ready) return -1;
+    set_globals(p, threads);
     const long int NBatch[2] = {p->nx, p->ny / 2 + 1};
     AllocateMemory(NBatch, &g_int);
     InitializeFFTWPlans(g_N);
@@ -179,4 +184,40 @@ void ref_system_measurables(double t, int iter, double* scalars, double* spectra
                       run_data->enst_flux_spect, run_data->enst_diss_spect, run_data->d_enrg_dt_spect,
                       run_data->enrg_flux_spect, run_data->enrg_diss_spect};
     for (int i = 0; i < 8; ++i) memcpy(spectra + (size_t)i * n, src[i], sizeof(double) * (size_t)n);
+}
+
+/* The reference's own time loop, SpectralSolve (Solver/src/solver.c:54-251),
+   from the initial condition named by p->u0 over [t0, T] with SAVE_EVERY =
+   p->save_every: it allocates, runs and frees everything itself, as under
+   main.c.  The state at each save (WriteDataToFile) is kept for
+   ref_saved_w_hat.  Once per process. */
+extern void (*shim_write_hook)(double t, long int iters);
+static double* g_saved = NULL;
+static double g_saved_t = 0.0;
+static long int g_saved_count = 0;
+
+static void keep_saved_state(double t, long int iters) {
+    (void)iters;
+    memcpy(g_saved, run_data->w_hat, sizeof(fftw_complex) * nspec());
+    g_saved_t = t;
+    g_saved_count++;
+}
+
+int ref_solve(const ref_params* p, int threads) {
+    if (g_ready) return -1;
+    set_globals(p, threads);
+    sys_vars->TRANS_ITERS_FLAG = 0;
+    g_saved = (double*)calloc(2 * nspec(), sizeof(double));
+    if (!g_saved) return -2;
+    shim_write_hook = keep_saved_state;
+    g_ready = 1;
+    SpectralSolve();
+    shim_write_hook = 0;
+    return 0;
+}
+
+long int ref_saved_w_hat(double* out, double* t) {
+    if (g_saved) memcpy(out, g_saved, sizeof(double) * 2 * nspec());
+    *t = g_saved_t;
+    return g_saved_count;
 }
