@@ -314,6 +314,84 @@ ns2d_status rhs_impl(ns2d_handle* h, const void* src, bool src_is_state) {
     return NS2D_OK;
 }
 
+// RK5DPStep (Solver/src/solver.c:360-570) as the reference intends it: seven
+// stages k_s = N(X_s) - D X_s with X_s = y0 + dt sum_r a_sr k_r (Butcher table
+// of solver.c:33-42), y5 into the state, and the RMS of the embedded error
+// scaled by DP_ABS_TOL + DP_REL_TOL max(|y0|, |y5|) (data_types.h:137-141).
+// The shipped code does not compile (it names run_data->w_hat_last and reads an
+// uninitialised err_sum); this is the corrected form.
+template <typename Real>
+ns2d_status dp5_step_impl(ns2d_handle* h, double dt, double* err) {
+    using C = Cplx<Real>;
+    static const double A[6][6] = {
+        {0.2, 0, 0, 0, 0, 0},
+        {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+        {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+        {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+        {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+        {35.0 / 384.0, 0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+    if (!h->dp[0]) {
+        for (void*& p : h->dp) {
+            CK(h, cudaMalloc(&p, h->field_bytes));
+            CK(h, cudaMemsetAsync(p, 0, h->field_bytes, h->stream));
+        }
+        CK(h, cudaMalloc((void**)&h->dp_kptr, sizeof(void*) * 7));
+        CK(h, cudaMemcpy((void*)h->dp_kptr, h->dp, sizeof(void*) * 7, cudaMemcpyHostToDevice));
+    }
+    compute_forcing(h, dt);
+    const bool euler = h->p.system == NS2D_EULER;
+    const int branch = euler ? 4 : resolve_branch(h, false);
+    void* y0 = h->dp[7];
+    void* x = h->dp[8];
+    CK(h, cudaMemcpyAsync(y0, h->state, h->field_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    for (int s = 0; s < 7; ++s) {
+        const void* xs = y0;
+        if (s > 0) {
+            DpCoef cf{};
+            cf.n = s;
+            for (int r = 0; r < s; ++r) cf.c[r] = A[s - 1][r];
+            const C* k[6];
+            for (int r = 0; r < 6; ++r) k[r] = (const C*)h->dp[r];
+            dp_combine_kernel<Real><<<296, 256, 0, h->stream>>>((C*)x, (const C*)y0, k[0], k[1], k[2], k[3], k[4],
+                                                               k[5], cf, dt, h->nx, h->nyf, h->ldc);
+            h->launches++;
+            xs = x;
+        }
+        ColArgs<Real> a;
+        fill_common<Real>(h, a, branch);
+        a.src = (const C*)xs;
+        launch_col<Real>(h, COL_P1, a);
+        launch_row<Real>(h);
+        fill_common<Real>(h, a, branch);
+        a.src = (const C*)h->nl;
+        a.rhs_store = (C*)h->dp[s];
+        a.conj_mode = 0;
+        a.lin_stage = euler ? 0 : 2;
+        a.xin = (const C*)xs;
+        launch_col<Real>(h, COL_RHS, a);
+    }
+    DpCoef b5{}, b4{};
+    const double B5[7] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
+    const double B4[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0, -92097.0 / 339200.0,
+                          187.0 / 2100.0, 1.0 / 40.0};
+    for (int r = 0; r < 7; ++r) {
+        b5.c[r] = B5[r];
+        b4.c[r] = B4[r];
+    }
+    b5.n = b4.n = 7;
+    dp_final_kernel<Real><<<296, 256, 0, h->stream>>>((C*)h->state, (const C*)y0, (const C* const*)h->dp_kptr, b5, b4,
+                                                     dt, 1e-7, 1e-7, h->nx, h->nyf, h->ldc, h->dpart);
+    h->launches++;
+    CKL(h);
+    double part[296];
+    CK(h, cudaMemcpyAsync(part, h->dpart, sizeof(part), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    double sum = 0.0;
+    for (int b = 0; b < 296; ++b) sum += part[b];
+    *err = std::sqrt(sum / (double)(h->nx * h->nyf));
+    return NS2D_OK;
+}
+
 // c2r of up to two spectral fields to x-space (f[0], f[1]) followed by a row
 // pass with a reduction or a store.
 template <typename Real>
@@ -419,6 +497,9 @@ void free_all(ns2d_handle* h) {
                     h->dstatus, h->dio, h->ddiag, h->dpart, h->cn};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (void* p : h->dp)
+        if (p) cudaFree(p);
+    if (h->dp_kptr) cudaFree((void*)h->dp_kptr);
 }
 
 template <typename Real>
@@ -1088,6 +1169,14 @@ ns2d_status ns2d_step_async(ns2d_handle* h, int32_t nsteps, double dt) {
         if (s) return s;
     }
     return NS2D_OK;
+}
+
+ns2d_status ns2d_dp5_step(ns2d_handle* h, double dt, double* err) {
+    if (!h || !err || !(dt > 0.0)) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    ns2d_status s = DISPATCH(h, dp5_step_impl, h, dt, err);
+    if (s) return s;
+    return check_status(h);
 }
 
 ns2d_status ns2d_check(ns2d_handle* h) {

@@ -238,4 +238,79 @@ __global__ void conj_kernel(typename Cx<Real>::T* state, int ldc, const typename
     state[(size_t)i * ldc] = cconj(src[(long long)(-kx) * src_stride]);
 }
 
+// Dormand-Prince 5(4) (RK5DPStep, Solver/src/solver.c:360-570, corrected).
+struct DpCoef {
+    double c[7];
+    int n;
+};
+
+// Stage input X = y0 + dt sum_{r < n} c_r k_r over the valid columns.
+template <typename Real>
+__global__ void dp_combine_kernel(typename Cx<Real>::T* __restrict__ x, const typename Cx<Real>::T* __restrict__ y0,
+                                  const typename Cx<Real>::T* k0, const typename Cx<Real>::T* k1,
+                                  const typename Cx<Real>::T* k2, const typename Cx<Real>::T* k3,
+                                  const typename Cx<Real>::T* k4, const typename Cx<Real>::T* k5, DpCoef cf,
+                                  double dt, int nx, int nyf, int ldc) {
+    using C = typename Cx<Real>::T;
+    const C* ks[6] = {k0, k1, k2, k3, k4, k5};
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const size_t o = (size_t)(q / nyf) * ldc + (size_t)(q % nyf);
+        double ar = 0.0, ai = 0.0;
+        for (int r = 0; r < cf.n; ++r) {
+            const C v = ks[r][o];
+            ar += cf.c[r] * (double)v.x;
+            ai += cf.c[r] * (double)v.y;
+        }
+        const C y = y0[o];
+        x[o] = cmake<C>((Real)((double)y.x + dt * ar), (Real)((double)y.y + dt * ai));
+    }
+}
+
+// Fifth-order solution y5 into the state (zero mean) and the embedded error
+// sum_j (|y5 - y4| / (atol + rtol max(|y0|, |y5|)))^2, one FP64 partial per block.
+template <typename Real>
+__global__ void __launch_bounds__(256) dp_final_kernel(typename Cx<Real>::T* __restrict__ state,
+                                                       const typename Cx<Real>::T* __restrict__ y0,
+                                                       const typename Cx<Real>::T* const* __restrict__ k,
+                                                       DpCoef b5, DpCoef b4, double dt, double atol, double rtol,
+                                                       int nx, int nyf, int ldc, double* partials) {
+    using C = typename Cx<Real>::T;
+    const long long n = (long long)nx * nyf;
+    double acc = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), j = (int)(q % nyf);
+        const size_t o = (size_t)i * ldc + j;
+        if (i == 0 && j == 0) {
+            state[o] = cmake<C>(0, 0);
+            continue;
+        }
+        double s5r = 0.0, s5i = 0.0, s4r = 0.0, s4i = 0.0;
+        for (int r = 0; r < 7; ++r) {
+            const C v = k[r][o];
+            s5r += b5.c[r] * (double)v.x;
+            s5i += b5.c[r] * (double)v.y;
+            s4r += b4.c[r] * (double)v.x;
+            s4i += b4.c[r] * (double)v.y;
+        }
+        const C y = y0[o];
+        const double y5r = (double)y.x + dt * s5r, y5i = (double)y.y + dt * s5i;
+        const double y4r = (double)y.x + dt * s4r, y4i = (double)y.y + dt * s4i;
+        const double sc = atol + rtol * fmax(hypot((double)y.x, (double)y.y), hypot(y5r, y5i));
+        const double e = hypot(y5r - y4r, y5i - y4i) / sc;
+        acc += e * e;
+        state[o] = cmake<C>((Real)y5r, (Real)y5i);
+    }
+    __shared__ double red[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        partials[blockIdx.x] = tot;
+    }
+}
+
 }  // namespace ns2d

@@ -63,6 +63,9 @@ struct ns2d_handle {
     // adjoint's own buffers (adjoint.cu)
     void* cap_step = nullptr;
     ns2d::AdjointState* adj = nullptr;
+    // Dormand-Prince stages k0..k6, y0 and the stage input (allocated on first use)
+    void* dp[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const void** dp_kptr = nullptr;  // device array of the seven stage pointers
     // one RK4/RK4CN step captured as a CUDA graph for fixed-dt stepping
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;

@@ -286,6 +286,12 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             }
             // forcing (solver.c:1022-1027)
             if (a.has_force && i == a.force_i && ky == a.force_j) r = cadd(r, a.force_val);
+            if constexpr (MODE == COL_RHS) {
+                // stage derivative with the explicit linear term (Dormand-Prince
+                // stages): r -= bracket(|k|^2) X, X the RHS input
+                if (a.lin_stage == 2 && a.xin && k2 != 0)
+                    r = csub(r, cscale(a.xin[(size_t)i * ldc + kyc], (Real)lin_bracket(a.lin, (double)k2)));
+            }
             if (a.rhs_store && valid) a.rhs_store[(size_t)i * ldc + ky] = r;
             // ForceConjugacy side effect on the state (solver.c:1031, 2096-2103)
             C w = cmake<C>(0, 0);

@@ -94,6 +94,13 @@ class Solver:
     def ab4_step(self, dt, iters):
         self._ck(self.L.ns2d_ab4_step(self.h, dt, iters))
 
+    def dp5_step(self, dt):
+        """One Dormand-Prince 5(4) trial step (RK5DPStep, corrected); returns
+        the scaled error estimate."""
+        e = C.c_double()
+        self._ck(self.L.ns2d_dp5_step(self.h, dt, C.byref(e)))
+        return e.value
+
     def step_n(self, n, dt):
         self._ck(self.L.ns2d_step_n(self.h, n, dt))
 

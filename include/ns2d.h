@@ -150,6 +150,16 @@ ns2d_status ns2d_rk4_step(ns2d_handle* h, double dt);
    1-based iteration counter: iters <= 3 take RK4CN start-up steps. */
 ns2d_status ns2d_ab4_step(ns2d_handle* h, double dt, int32_t iters);
 
+/* RK5DPStep (Solver/src/solver.c:360-570; solver.h:33): one Dormand-Prince
+   5(4) trial step of dt, in place (the state becomes the fifth-order solution),
+   *err = RMS over the half spectrum of |y5 - y4| / (1e-7 + 1e-7 max(|y0|, |y5|))
+   (DP_ABS_TOL, DP_REL_TOL, data_types.h:137-141), accumulated in FP64.  The
+   linear term is explicit in every stage.  The shipped routine does not compile
+   (w_hat_last, an uninitialised err_sum) and its driver's accept/retry test is
+   inverted (solver.c:153-171); this is the corrected step, and accepting or
+   retrying is the caller's (dt_new = dt min(1.5, max(0.01, 0.8 err^-1/5))). */
+ns2d_status ns2d_dp5_step(ns2d_handle* h, double dt, double* err);
+
 /* nsteps fixed-dt steps of the configured integrator without host round trips
    (the loop body of SpectralSolve, solver.c:142-236, minus saving). */
 ns2d_status ns2d_step_n(ns2d_handle* h, int32_t nsteps, double dt);
