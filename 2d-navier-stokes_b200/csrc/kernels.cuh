@@ -102,6 +102,8 @@ struct ColArgs {
     const double2* cn;   // COL_FINAL, CN schemes: per-mode ((2-D)/(2+D), 2dt/(2+D)), stride ldc
     double inv_nxny;     // 1/(Nx Ny)
     int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
+    int next_p1;         // COL_FINAL: also the derived spectra of the new state and their
+                         // inverse x-FFTs (the next step's first column pass)
     int ntiles;          // number of column tiles of this field
     int* status;         // [0] status bits (kernels return early when set), [1] completed steps
 };
@@ -351,6 +353,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                         const double2 f = a.cn[(size_t)i * ldc + kyc];
                         wn = cadd(cscale(w, (Real)f.x), cscale(tot, (Real)f.y));
                     }
+                    pre0[q] = wn;  // source of the next step's derived spectra (next_p1)
                     if (valid) {
                         a.state[(size_t)i * ldc + ky] = wn;
                         const double mag = fabs((double)wn.x) + fabs((double)wn.y);
@@ -393,7 +396,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 if (tile == 0) atomicAdd(a.status + 1, 1);  // completed steps
             }
             __syncthreads();
-            return;
+            if (!a.next_p1) return;
         }
         if constexpr (MODE == COL_RHS) return;
     }

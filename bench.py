@@ -41,12 +41,13 @@ DT = 2.5e-4
 NU_H = 2e-40
 WORKLOAD = "kolmogorov_1024_fp64_rk4cn"
 S_BYTES = 16 * N * (N // 2 + 1)  # one FP64 half spectrum
-# algorithmic bytes per launch, in units of S, per kernel class:
-# 0 column pass P1 (read 1, write 4), 1 column pass with stage combine (read
-# n, w, acc; write acc + 4 fields: 8; stage 1 has no acc read: 7), 2 final
-# column pass (read n, w, acc; write w: 4), 3 row pass (read 4, write 1).
+# algorithmic bytes per launch, in units of S, per kernel class: 0 first column
+# pass (read w, write 4 fields: 5), 1 column pass with stage combine (read n,
+# w, acc; write acc + 4 fields: 8; stage 1 has no acc read: 7; mean 23/3),
+# 2 final column pass of the fixed-dt loop (read n, w, acc, CN table; write w
+# and the next step's 4 fields: 9), 3 row pass (read 4, write 1: 5).
 CLASS_NAMES = ["col_p1", "col_stage", "col_final", "row", "other"]
-CLASS_BYTES_PER_STEP = {0: 5, 1: 7 + 8 + 8, 2: 4, 3: 4 * 5}
+CLASS_BYTES_PER_LAUNCH = {0: 5.0, 1: 23.0 / 3.0, 2: 9.0, 3: 5.0}
 MODEL_BYTES_PER_STEP = 58  # the 2-pass minimal model (58 S per RK4 step)
 
 
@@ -387,18 +388,21 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * ke / float(te.item())
 
-    # FP32 batched ensemble (same process, same GPU)
-    ens_v, ens_ms, ens_grids, ens_launches, ens_z = ensemble_bench(stream, flush, args.ens_steps, args.warmup, rank)
-    te2 = torch.tensor([ens_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te2, op=dist.ReduceOp.MAX)
-    ens_total = world * 1e3 / float(te2.item())
+    full = args.only != "plain"
+    if full:
+        # FP32 batched ensemble (same process, same GPU)
+        ens_v, ens_ms, ens_grids, ens_launches, ens_z = ensemble_bench(stream, flush, args.ens_steps, args.warmup,
+                                                                       rank)
+        te2 = torch.tensor([ens_ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te2, op=dist.ReduceOp.MAX)
+        ens_total = world * 1e3 / float(te2.item())
 
-    # discrete adjoint at 512^2, FP64 and FP32 (same process, same GPU)
-    from ns2d import abi as _abi
-    adj64 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP64)
-    adj32 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP32, g_ref=adj64.pop("gradient"))
-    adj = [adj64, adj32]
+        # discrete adjoint at 512^2, FP64 and FP32 (same process, same GPU)
+        from ns2d import abi as _abi
+        adj64 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP64)
+        adj32 = adjoint_bench(stream, args.adj_steps, rank, _abi.FP32, g_ref=adj64.pop("gradient"))
+        adj = [adj64, adj32]
 
     if rank != 0:
         s.close()
@@ -407,7 +411,7 @@ def run_gpu(args, rank, world, local_rank):
     # roofline of the dominant kernel class
     peak, peak_kind = peaks()
     dom = int(np.argmax(kms[:4]))
-    per_launch_bytes = CLASS_BYTES_PER_STEP[dom] * S_BYTES / (kn[dom] / args.steps)
+    per_launch_bytes = CLASS_BYTES_PER_LAUNCH[dom] * S_BYTES
     avg_ms = kms[dom] / kn[dom]
     achieved = per_launch_bytes / (avg_ms * 1e-3) / 1e9
     step_ms = ms_max / args.steps
@@ -428,19 +432,20 @@ def run_gpu(args, rank, world, local_rank):
                 "call": "ns2d_rk4_step_host"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
-        "fp32_batched": {
+    }
+    if full:
+        line["fp32_batched"] = {
             "workload": "ensemble 32x128^2 + 24x256^2 + 8x512^2 (4 x 1024^2 points), FP32 RK4CN, nu=1e-3, dt=1e-3",
             "ensemble_steps_per_s": ens_total, "ms_per_step": float(te2.item()),
             "equiv_1024_steps_per_s": 4.0 * ens_total, "ratio_vs_fp64_plain": 4.0 * ens_total / value,
             "tuned_grids": {"col": ens_grids[0], "row": ens_grids[1]}, "gpu_launches": int(ens_launches),
             "enstrophy_sample": ens_z, "launches_per_step": 9,
-        },
-        "adjoint": {
+        }
+        line["adjoint"] = {
             "workload": f"gradient of Z(T) w.r.t. w0, {ADJ_N}^2, nu=1e-3, RK4CN dt={ADJ_DT}, {args.adj_steps} steps, "
                         f"checkpoints every {ADJ_EVERY} steps with stage recomputation",
             "adjoint_over_forward": adj[0]["adjoint_over_forward"], "runs": adj,
-        },
-    }
+        }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, st, el = cpu_reference(1000, 1, threads, budget_s=args.cpu_seconds)
@@ -463,8 +468,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--adj-steps", type=int, default=2000)
-    ap.add_argument("--only", choices=["ensemble", "adjoint"], default=None,
-                    help="run one part alone and print its JSON object (profiling runs)")
+    ap.add_argument("--only", choices=["plain", "ensemble", "adjoint"], default=None,
+                    help="one part alone (profiling runs): plain = the 1024^2 FP64 line without the "
+                         "ensemble and adjoint parts; ensemble / adjoint print that part's JSON object")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -473,7 +479,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
-    if args.only:
+    if args.only in ("ensemble", "adjoint"):
         return run_part(args, local_rank)
     if world > 1:
         import datetime
