@@ -32,6 +32,7 @@
 
 #include "data_types.h"
 #include "solver.h"
+#include "force.h"
 #include "ns2d.h"
 
 static ns2d_handle* g_ns2d = NULL;
@@ -92,13 +93,21 @@ static ns2d_handle* ns2d_compat_handle(void) {
     return g_ns2d;
 }
 
-/* RK4Step (solver.c:625): one step of run_data->w_hat, in place. */
+/* RK4Step (solver.c:625): one step of run_data->w_hat, in place.  The host
+   side effects of the replaced body are kept: the forcing values of this step
+   (ComputeForcing, solver.c:650), which ComputeSystemMeasurables reads, and
+   the `=` in the viscous-branch test that sets HYPER_VISC_FLAG whenever Ekman
+   drag is off (solver.c:675, 843). */
 void RK4Step(const double dt, const long int* N, const ptrdiff_t local_Nx, Int_data_struct* Int_data) {
     (void)N;
     (void)local_Nx;
     (void)Int_data;
     ns2d_handle* h = ns2d_compat_handle();
+    ComputeForcing(dt);
     ns2d_compat_check(ns2d_rk4_step_host(h, (double*)run_data->w_hat, dt), "RK4Step");
+#if !defined(__EULER)
+    if (sys_vars->EKMN_DRAG_FLAG != EKMN_DRAG) sys_vars->HYPER_VISC_FLAG = HYPER_VISC;
+#endif
 }
 
 /* ForceConjugacy (solver.c:2074): the ky = 0 entries of run_data->w_hat with

@@ -200,6 +200,43 @@ __device__ __forceinline__ void derived_pair(int fp, int kx, int ky, C X, C& a, 
     b = cmake<C>(-sb * X.y, sb * X.x);
 }
 
+// Derived spectra of the stage input X (pre0, [N][TC] in shared memory) and
+// their four inverse x-FFTs into f0..f3, two at a time.  Out of line: every
+// column pass that ends this way (first pass, stage passes, the final pass of
+// the fixed-dt loop) runs this one compiled body, so the next stage's input
+// fields are bit-for-bit the same whichever pass produced them, and the
+// transform code is held once in the instruction cache.
+template <typename Real, int N, int TC>
+__device__ __noinline__ void derived_ifft(const typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
+                                          typename Cx<Real>::T* f0, typename Cx<Real>::T* f1,
+                                          typename Cx<Real>::T* f2, typename Cx<Real>::T* f3, int ldc, int ky,
+                                          bool valid, int t, int c, TwSeed<typename Cx<Real>::T> seed) {
+    using C = typename Cx<Real>::T;
+    constexpr int T = Plan<N>::T;
+    constexpr int E = N / T;
+    C* outs[4] = {f0, f1, f2, f3};
+#pragma unroll 1
+    for (int fp = 0; fp < 4; fp += 2) {
+        C v[2][E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int i = t + T * m;
+            const int kx = (i <= N / 2) ? i : i - N;
+            derived_pair(fp, kx, ky, pre0[i * TC + c], v[0][m], v[1][m]);
+        }
+        fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
+        if (valid) {
+            C* __restrict__ o0 = outs[fp];
+            C* __restrict__ o1 = outs[fp + 1];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                o0[(size_t)(t + T * m) * ldc + ky] = v[0][m];
+                o1[(size_t)(t + T * m) * ldc + ky] = v[1][m];
+            }
+        }
+    }
+}
+
 // Column pass on tile `tile` (ky columns tile*TC .. tile*TC+TC-1), by the T*TC
 // threads of a block, thread (t, c) with c = threadIdx.x % TC.  Shared memory:
 // ColSmem::bytes().  Ends with the block synchronised (the shared memory may be
@@ -401,29 +438,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
         if constexpr (MODE == COL_RHS) return;
     }
 
-    // derived spectra of the stage input and four inverse x-FFTs, two at a
-    // time (one copy of the transform code serves both pairs)
-    C* outs[4] = {a.f0, a.f1, a.f2, a.f3};
-#pragma unroll 1
-    for (int fp = 0; fp < 4; fp += 2) {
-        C v[2][E];
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int i = t + T * m;
-            const int kx = (i <= N / 2) ? i : i - N;
-            derived_pair(fp, kx, ky, pre0[i * TC + c], v[0][m], v[1][m]);
-        }
-        fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
-        if (valid) {
-            C* __restrict__ o0 = outs[fp];
-            C* __restrict__ o1 = outs[fp + 1];
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                o0[(size_t)(t + T * m) * ldc + ky] = v[0][m];
-                o1[(size_t)(t + T * m) * ldc + ky] = v[1][m];
-            }
-        }
-    }
+    derived_ifft<Real, N, TC>(pre0, sm, a.f0, a.f1, a.f2, a.f3, ldc, ky, valid, t, c, seed);
 }
 
 // Column pass of one field.  Grid: ceil(nyf / TC) blocks; block: T * TC threads.

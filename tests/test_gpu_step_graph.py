@@ -28,9 +28,8 @@ def test_graph_replay_matches_eager_steps(n, quirks):
         b.step_n(j - i, dts[i])
         i = j
     assert np.array_equal(a.get_w_hat(), b.get_w_hat())
-    la = a.launch_count
-    lb = b.launch_count
-    assert lb >= la  # graph replays are counted as their kernels
+    # graph replays count their kernels; the fused loop launches fewer
+    assert 0 < b.launch_count <= a.launch_count
 
 
 def test_step_async_then_timing_mode():
