@@ -200,7 +200,7 @@ ns2d_status ensure_cn(ns2d_handle* h, double dt, int branch) {
 // One RK4 / RK4CN step (RK4Step, Solver/src/solver.c:625-873).  If rk1_out is
 // non-null the stage-1 RHS is stored there (AB4 start-up, solver.c:283).
 template <typename Real>
-ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out, bool skip_p1 = false, bool next_p1 = false) {
+ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out) {
     using C = Cplx<Real>;
     compute_forcing(h, dt);
     const bool euler = h->p.system == NS2D_EULER;
@@ -216,11 +216,9 @@ ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out, bool skip_p1
     const bool conj_quirk = quirk(h, NS2D_QUIRK_CONJ_STATE);
 
     ColArgs<Real> a;
-    if (!skip_p1) {  // else f[0..3] already hold the state's derived spectra
-        fill_common<Real>(h, a, branch);
-        a.src = (const C*)h->state;
-        launch_col<Real>(h, COL_P1, a);
-    }
+    fill_common<Real>(h, a, branch);
+    a.src = (const C*)h->state;
+    launch_col<Real>(h, COL_P1, a);
     for (int s = 1; s <= 4; ++s) {
         launch_row<Real>(h, s);
         fill_common<Real>(h, a, branch);
@@ -246,7 +244,6 @@ ns2d_status rk4_step_impl(ns2d_handle* h, double dt, void* rk1_out, bool skip_p1
             launch_col<Real>(h, COL_STAGE, a);
         } else {
             a.scheme = explicit_rk4 ? 1 : 0;
-            a.next_p1 = next_p1 ? 1 : 0;
             if (!explicit_rk4) {
                 ns2d_status s2 = ensure_cn(h, dt, branch);
                 if (s2) return s2;
@@ -570,18 +567,15 @@ void drop_graph(ns2d_handle* h) {
     if (h->timed_graph) cudaGraphExecDestroy(h->timed_graph);
     h->timed_graph = nullptr;
     h->timed_branch = -1;
-    for (auto& g : h->fused_graph) {
-        if (g) cudaGraphExecDestroy(g);
-        g = nullptr;
-    }
+
 }
 
 // Captures the launches of one RK4/RK4CN step (recorded, not executed).
-ns2d_status capture_step(ns2d_handle* h, double dt, bool skip_p1, cudaGraphExec_t* out) {
+ns2d_status capture_step(ns2d_handle* h, double dt, cudaGraphExec_t* out) {
     const int64_t l0 = h->launches;
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr, skip_p1, true);
+    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = l0;
     if (s) {
@@ -599,65 +593,49 @@ ns2d_status capture_step(ns2d_handle* h, double dt, bool skip_p1, cudaGraphExec_
 }
 
 // One fixed-dt RK4/RK4CN step for the time loops (ns2d_step_n, ns2d_step_async,
-// the adjoint's record).  Each step's final column pass also produces the next
-// step's derived spectra (next_p1), so a step that follows another loop step
-// with no launch in between skips its first column pass.  The first step with
-// a given dt runs eagerly (it settles the operator branch and the CN table);
-// the step is then captured once per form (with and without the first column
-// pass) as a CUDA graph and replayed.  With kernel timing on, separate graphs
-// carry an event pair around every launch, read back after each replay.
-// Stage capture for the adjoint uses the eager form.
+// the adjoint's record).  The first step with a given dt runs eagerly (it
+// settles the operator branch and the CN table); the step is then captured
+// once as a CUDA graph of its nine launches and replayed for the following
+// steps.  With kernel timing on, a second graph carries an event pair around
+// every launch and is read back after each replay.  Stage capture for the
+// adjoint uses the eager form.
 ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
     if (h->cap_step) return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
-    const bool skip_p1 = h->p1_ready && h->p1_mark == h->launches;
     int hf = h->hyper_flag;
     const int branch = (h->p.system == NS2D_EULER && h->p.integrator != NS2D_RK4)
                            ? 4
                            : ns2d::resolve_branch(hf, h->p.ekmn_drag_flag, quirk(h, NS2D_QUIRK_HYPER_LATCH));
     const bool settled = (hf == h->hyper_flag) && h->cn_dt == dt && h->cn_branch == branch;
+    cudaGraphExec_t* gx = h->timing ? &h->timed_graph : &h->step_graph;
     double* gdt = h->timing ? &h->timed_dt : &h->graph_dt;
     int* gbr = h->timing ? &h->timed_branch : &h->graph_branch;
-    cudaGraphExec_t* full = h->timing ? &h->timed_graph : &h->step_graph;
-    cudaGraphExec_t* fused = &h->fused_graph[h->timing ? 1 : 0];
-    if (!(*gdt == dt && *gbr == branch && settled)) {
-        for (cudaGraphExec_t* g : {full, fused}) {
-            if (*g) cudaGraphExecDestroy(*g);
-            *g = nullptr;
-        }
-        *gdt = 0.0;
-        *gbr = -1;
-        // this call's step, eagerly
-        ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr, skip_p1, true);
+    const int set = h->timing ? 1 : 0;
+    if (!(*gx && *gdt == dt && *gbr == branch && settled)) {
+        if (*gx) cudaGraphExecDestroy(*gx);
+        *gx = nullptr;
+        ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);  // this call's step
         if (s) return s;
-        h->p1_ready = true;
-        h->p1_mark = h->launches;
+        h->capturing_timed = h->timing;
+        h->gev_n = 0;
+        h->gev_set = set;
+        s = capture_step(h, dt, gx);
+        h->capturing_timed = false;
+        if (s) return s;
+        h->gev_n_of[set] = h->gev_n;
         *gdt = dt;
         *gbr = h->cn_branch;
         return NS2D_OK;
     }
-    cudaGraphExec_t* gx = skip_p1 ? fused : full;
-    if (!*gx) {
-        h->capturing_timed = h->timing;
-        h->gev_n = 0;
-        h->gev_set = skip_p1 ? 1 : 0;
-        ns2d_status s = capture_step(h, dt, skip_p1, gx);
-        h->capturing_timed = false;
-        if (s) return s;
-        if (h->timing) h->gev_n_of[skip_p1 ? 1 : 0] = h->gev_n;
-    }
     cudaError_t e = cudaGraphLaunch(*gx, h->stream);
     if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
-    h->launches += skip_p1 ? 8 : 9;
-    h->p1_ready = true;
-    h->p1_mark = h->launches;
+    h->launches += 9;
     if (h->timing) {
         CK(h, cudaStreamSynchronize(h->stream));
-        const int g = skip_p1 ? 1 : 0;
-        for (int k = 0; k < h->gev_n_of[g]; ++k) {
+        for (int k = 0; k < h->gev_n_of[set]; ++k) {
             float ms = 0.f;
-            CK(h, cudaEventElapsedTime(&ms, h->gev_g[g][k][0], h->gev_g[g][k][1]));
-            h->t_ms[h->gev_cls_g[g][k]] += ms;
-            h->t_n[h->gev_cls_g[g][k]] += 1;
+            CK(h, cudaEventElapsedTime(&ms, h->gev_g[set][k][0], h->gev_g[set][k][1]));
+            h->t_ms[h->gev_cls_g[set][k]] += ms;
+            h->t_n[h->gev_cls_g[set][k]] += 1;
         }
     }
     return NS2D_OK;

@@ -75,12 +75,7 @@ struct ns2d_handle {
     double timed_dt = 0.0;
     int timed_branch = -1;
     bool capturing_timed = false;
-    // the fixed-dt loop fuses each step's final column pass with the next
-    // step's first: f[0..3] then hold the derived spectra of the state, valid
-    // while no other launch has run since (launch counter mark)
-    bool p1_ready = false;
-    int64_t p1_mark = -1;
-    cudaGraphExec_t fused_graph[2] = {nullptr, nullptr};  // [timing]
+
     int gev_n = 0;
     int gev_set = 0;                 // event set being captured: [0] full step, [1] fused step
     int gev_n_of[2] = {0, 0};

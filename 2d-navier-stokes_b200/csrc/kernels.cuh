@@ -102,8 +102,6 @@ struct ColArgs {
     const double2* cn;   // COL_FINAL, CN schemes: per-mode ((2-D)/(2+D), 2dt/(2+D)), stride ldc
     double inv_nxny;     // 1/(Nx Ny)
     int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
-    int next_p1;         // COL_FINAL: also the derived spectra of the new state and their
-                         // inverse x-FFTs (the next step's first column pass)
     int ntiles;          // number of column tiles of this field
     int* status;         // [0] status bits (kernels return early when set), [1] completed steps
 };
@@ -201,13 +199,10 @@ __device__ __forceinline__ void derived_pair(int fp, int kx, int ky, C X, C& a, 
 }
 
 // Derived spectra of the stage input X (pre0, [N][TC] in shared memory) and
-// their four inverse x-FFTs into f0..f3, two at a time.  Out of line: every
-// column pass that ends this way (first pass, stage passes, the final pass of
-// the fixed-dt loop) runs this one compiled body, so the next stage's input
-// fields are bit-for-bit the same whichever pass produced them, and the
-// transform code is held once in the instruction cache.
+// their four inverse x-FFTs into f0..f3, two at a time (one copy of the
+// transform code serves both pairs).
 template <typename Real, int N, int TC>
-__device__ __noinline__ void derived_ifft(const typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
+__device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
                                           typename Cx<Real>::T* f0, typename Cx<Real>::T* f1,
                                           typename Cx<Real>::T* f2, typename Cx<Real>::T* f3, int ldc, int ky,
                                           bool valid, int t, int c, TwSeed<typename Cx<Real>::T> seed) {
@@ -390,7 +385,6 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                         const double2 f = a.cn[(size_t)i * ldc + kyc];
                         wn = cadd(cscale(w, (Real)f.x), cscale(tot, (Real)f.y));
                     }
-                    pre0[q] = wn;  // source of the next step's derived spectra (next_p1)
                     if (valid) {
                         a.state[(size_t)i * ldc + ky] = wn;
                         const double mag = fabs((double)wn.x) + fabs((double)wn.y);
@@ -433,7 +427,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 if (tile == 0) atomicAdd(a.status + 1, 1);  // completed steps
             }
             __syncthreads();
-            if (!a.next_p1) return;
+            return;
         }
         if constexpr (MODE == COL_RHS) return;
     }

@@ -44,10 +44,10 @@ S_BYTES = 16 * N * (N // 2 + 1)  # one FP64 half spectrum
 # algorithmic bytes per launch, in units of S, per kernel class: 0 first column
 # pass (read w, write 4 fields: 5), 1 column pass with stage combine (read n,
 # w, acc; write acc + 4 fields: 8; stage 1 has no acc read: 7; mean 23/3),
-# 2 final column pass of the fixed-dt loop (read n, w, acc, CN table; write w
-# and the next step's 4 fields: 9), 3 row pass (read 4, write 1: 5).
+# 2 final column pass (read n, w, acc, CN table; write w: 5), 3 row pass (read
+# 4, write 1: 5).
 CLASS_NAMES = ["col_p1", "col_stage", "col_final", "row", "other"]
-CLASS_BYTES_PER_LAUNCH = {0: 5.0, 1: 23.0 / 3.0, 2: 9.0, 3: 5.0}
+CLASS_BYTES_PER_LAUNCH = {0: 5.0, 1: 23.0 / 3.0, 2: 5.0, 3: 5.0}
 MODEL_BYTES_PER_STEP = 58  # the 2-pass minimal model (58 S per RK4 step)
 
 
