@@ -222,9 +222,9 @@ ns2d_status create_t(ns2d_ensemble* e) {
     cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, dev);
     // default persistent grids: every item in one wave where it fits
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_col_kernel<Real, COL_STAGE>, 128, e->col_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_col_kernel<Real, COL_STAGE>, kEnsThreads, e->col_smem);
     e->col_grid = std::max(1, std::min(e->n_col_items, e->nsm * std::max(1, per_sm)));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_row_kernel<Real>, 128, e->row_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_row_kernel<Real>, kEnsThreads, e->row_smem);
     e->row_grid = std::max(1, std::min(e->n_row_items, e->nsm * std::max(1, per_sm)));
     ECK(e, cudaStreamSynchronize(e->stream));
     return NS2D_OK;
@@ -258,20 +258,20 @@ ns2d_status step_t(ns2d_ensemble* e, double dt) {
     st.conj_quirk = (e->p.quirks & NS2D_QUIRK_CONJ_STATE) ? 1 : 0;
     st.status = e->status;
     st.stage = 0;
-    ens_col_kernel<Real, COL_P1><<<e->col_grid, 128, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+    ens_col_kernel<Real, COL_P1><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
     e->launches++;
     for (int s = 1; s <= 4; ++s) {
-        ens_row_kernel<Real><<<e->row_grid, 128, e->row_smem, e->stream>>>(mb, e->row_items, e->n_row_items, e->status);
+        ens_row_kernel<Real><<<e->row_grid, kEnsThreads, e->row_smem, e->stream>>>(mb, e->row_items, e->n_row_items, e->status);
         e->launches++;
         st.stage = s;
         st.b_cur = explicit_rk4 ? B_ex[s - 1] : B_cn[s - 1];
         if (s < 4) {
             st.a_next = A[s - 1];
             st.first = (s == 1);
-            ens_col_kernel<Real, COL_STAGE><<<e->col_grid, 128, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+            ens_col_kernel<Real, COL_STAGE><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
         } else {
             st.scheme = explicit_rk4 ? 1 : 0;
-            ens_col_kernel<Real, COL_FINAL><<<e->col_grid, 128, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+            ens_col_kernel<Real, COL_FINAL><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
         }
         e->launches++;
     }

@@ -2,20 +2,24 @@
 // together: one launch per pass covers every member.  A launch walks a list
 // of work items (member, tile) with a persistent grid; each item runs the same
 // column or row body as the single-trajectory kernels, instantiated for the
-// member's grid size.  All bodies use 128-thread blocks, so one launch can mix
-// sizes.
+// member's grid size.  All bodies use blocks of kEnsThreads threads, so one
+// launch can mix sizes.
 #pragma once
 #include "kernels.cuh"
 
 namespace ns2d {
 
-// Tile shapes of the ensemble kernels: 128 threads for every size.
+// Block size of the ensemble kernels (every member size), and the tile shapes
+// it gives.  256 threads measured 12 % faster than 128 on the 64-member FP32
+// benchmark ensemble: the 512^2 members' column tiles grow from 2 to 4 columns
+// (32 B per row access in FP32), the 128^2 / 256^2 ones from 8 to 16.
+constexpr int kEnsThreads = 256;
 template <int N>
 struct EnsShape {
     static constexpr int T = Plan<N>::T;
-    static constexpr int TC = 128 / T;          // columns per column tile
-    static constexpr int PAIRS = 128 / (2 * T);  // row pairs per row block
-    static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= 64");
+    static constexpr int TC = kEnsThreads / T;          // columns per column tile
+    static constexpr int PAIRS = kEnsThreads / (2 * T);  // row pairs per row block
+    static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= kEnsThreads / 2");
 };
 
 #define NS2D_ENS_SIZES(X) X(64) X(128) X(256) X(512)
@@ -69,16 +73,16 @@ __device__ __forceinline__ void ens_apply_stage(ColArgs<Real>& a, const EnsMembe
     }
 }
 
-// Resident 128-thread blocks per SM the ensemble kernels are compiled for: four
-// in FP32 (at most 128 registers a thread), the register need of one FP64
-// body otherwise.
+// Resident blocks per SM the ensemble kernels are compiled for: two in FP32
+// (at most 128 registers a thread), the register need of one FP64 body
+// otherwise.
 template <typename Real>
 struct EnsMinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? 4 : 1;
+    static constexpr int value = sizeof(Real) == 4 ? 2 : 1;
 };
 
 template <typename Real, int MODE>
-__global__ void __launch_bounds__(128, EnsMinBlocks<Real>::value) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
+__global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, EnsStage st) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(st.status)) return;
@@ -100,7 +104,7 @@ __global__ void __launch_bounds__(128, EnsMinBlocks<Real>::value) ens_col_kernel
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(128, EnsMinBlocks<Real>::value) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
+__global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, int* status) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(status)) return;
