@@ -176,9 +176,17 @@ void launch_row(ns2d_handle* h, int stage = 0) {
     with_size<Real>(h->nx, [&](auto L) { decltype(L)::row(r, h->stream); });
 }
 
-// Forcing values for this step (ComputeForcing, Solver/src/force.c:516-581).
+// Forcing values for this step (ComputeForcing, Solver/src/force.c:516-581);
+// ZERO forcing kills its modes of the state instead.
 void compute_forcing(ns2d_handle* h, double dt) {
     (void)dt;
+    if (h->p.forcing == NS2D_FORCING_ZERO) {
+        if (h->fp32)
+            zero_modes_kernel<float><<<296, 256, 0, h->stream>>>((float2*)h->state, h->nx, h->nyf, h->ldc, h->p.force_k);
+        else
+            zero_modes_kernel<double><<<296, 256, 0, h->stream>>>((double2*)h->state, h->nx, h->nyf, h->ldc, h->p.force_k);
+        h->launches++;
+    }
     if (h->p.forcing == NS2D_FORCING_KOLM && h->forced) {
         // -0.5 * F * (k + 0 i)  (force.c:537)
         h->fre = -0.5 * h->p.force_scale * (double)h->p.force_k;
@@ -577,6 +585,7 @@ ns2d_status capture_step(ns2d_handle* h, double dt, cudaGraphExec_t* out) {
     CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->graph_kernels = (int)(h->launches - l0);
     h->launches = l0;
     if (s) {
         if (g) cudaGraphDestroy(g);
@@ -628,7 +637,7 @@ ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
     }
     cudaError_t e = cudaGraphLaunch(*gx, h->stream);
     if (e != cudaSuccess) return fail(h, NS2D_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
-    h->launches += 9;
+    h->launches += h->graph_kernels;
     if (h->timing) {
         CK(h, cudaStreamSynchronize(h->stream));
         for (int k = 0; k < h->gev_n_of[set]; ++k) {

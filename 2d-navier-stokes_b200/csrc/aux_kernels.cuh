@@ -238,6 +238,19 @@ __global__ void conj_kernel(typename Cx<Real>::T* state, int ldc, const typename
     state[(size_t)i * ldc] = cconj(src[(long long)(-kx) * src_stride]);
 }
 
+// ZERO forcing (ComputeForcing, Solver/src/force.c:527-533): every mode with
+// |kx| <= k or |ky| <= k of the state is set to zero (modes of force.c:436-501).
+template <typename Real>
+__global__ void zero_modes_kernel(typename Cx<Real>::T* state, int nx, int nyf, int ldc, int k) {
+    using C = typename Cx<Real>::T;
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), j = (int)(q % nyf);
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        if ((kx < 0 ? -kx : kx) <= k || j <= k) state[(size_t)i * ldc + j] = cmake<C>(0, 0);
+    }
+}
+
 // Dormand-Prince 5(4) (RK5DPStep, Solver/src/solver.c:360-570, corrected).
 struct DpCoef {
     double c[7];

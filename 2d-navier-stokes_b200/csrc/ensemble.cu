@@ -437,6 +437,7 @@ ns2d_status ns2d_ensemble_create(const ns2d_params* base, int32_t n_members, con
     if (!base || !sizes || !out || n_members < 1) return NS2D_ERR_INVALID;
     *out = nullptr;
     if (base->integrator != NS2D_RK4CN && base->integrator != NS2D_RK4) return NS2D_ERR_UNSUPPORTED;
+    if (base->forcing == NS2D_FORCING_ZERO) return NS2D_ERR_UNSUPPORTED;  // mode killing: single handles only
     if (base->precision != NS2D_FP64 && base->precision != NS2D_FP32) return NS2D_ERR_INVALID;
     for (int m = 0; m < n_members; ++m)
         if (!ens_size_ok(sizes[m])) return NS2D_ERR_UNSUPPORTED;

@@ -68,6 +68,7 @@ struct ns2d_handle {
     const void** dp_kptr = nullptr;  // device array of the seven stage pointers
     // one RK4/RK4CN step captured as a CUDA graph for fixed-dt stepping
     cudaGraphExec_t step_graph = nullptr;
+    int graph_kernels = 9;  // kernels in one captured step
     double graph_dt = 0.0;
     int graph_branch = -1;
     // the same with an event pair around every launch (kernel timing mode)

@@ -57,7 +57,9 @@ typedef enum ns2d_dealias { NS2D_DEALIAS_23 = 0, NS2D_DEALIAS_HOU_LI = 1 } ns2d_
 typedef enum ns2d_forcing {
     NS2D_FORCING_NONE = 0,
     NS2D_FORCING_KOLM = 1, /* "KOLM": one mode (kx=0, ky=force_k), value -F*n/2 */
-    NS2D_FORCING_ZERO = 2  /* "ZERO": listed modes set to 0 each step          */
+    NS2D_FORCING_ZERO = 2  /* "ZERO": modes with |kx| or |ky| <= force_k set to 0
+                              at the start of every step (force.c:436-533);
+                              single handles only                               */
 } ns2d_forcing;
 typedef enum ns2d_precision { NS2D_FP64 = 0, NS2D_FP32 = 1 } ns2d_precision;
 

@@ -126,11 +126,19 @@ void oracle_set_w_max_init(ns2d_oracle* o, double w) { o->w_max_init = w; }
 void oracle_set_w_hat(ns2d_oracle* o, const double* w) { memcpy(o->w_hat, w, o->ns * sizeof(cplx)); }
 void oracle_get_w_hat(const ns2d_oracle* o, double* w) { memcpy(w, o->w_hat, o->ns * sizeof(cplx)); }
 
-/* ComputeForcing: Solver/src/force.c:516-581 (KOLM, ZERO). */
+/* ComputeForcing: Solver/src/force.c:516-581 (KOLM, ZERO).  ZERO kills every
+   mode with |kx| <= force_k or |ky| <= force_k in the state (the modes chosen
+   at force.c:436-501, zeroed at :527-533); its forcing values stay 0. */
 void oracle_compute_forcing(ns2d_oracle* o, double dt) {
     (void)dt;
     if (o->p.forcing == NS2D_FORCING_KOLM && o->n_forced)
         o->forcing_val = -0.5 * o->p.force_scale * (o->p.force_k + 0.0 * I);
+    if (o->p.forcing == NS2D_FORCING_ZERO) {
+        for (int i = 0; i < o->nx; ++i)
+            for (int j = 0; j < o->nyf; ++j)
+                if (abs(o->kx[i]) <= o->p.force_k || abs(o->ky[j]) <= o->p.force_k)
+                    o->w_hat[(size_t)i * o->nyf + j] = 0.0;
+    }
 }
 
 /* Bracket of the linear operator D/dt (Solver/src/solver.c:839-856, also

@@ -50,6 +50,9 @@ def cases():
         # Nyquist row/column are populated; reference built with __DEALIAS_HOU_LI
         "houli32": ("houli", dict(nx=32, ny=32, nu=5e-4, dealias=abi.DEALIAS_HOU_LI, dt=1e-3),
                     ("decaying", 8, 6.0, None), [("rhs_state",), ("steps", 10, 1e-3), ("w_hat",)]),
+        # ZERO forcing: modes with |kx| <= 2 or |ky| <= 2 killed every step
+        "zero32_rk4cn": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, forcing=abi.FORCING_ZERO, force_k=2, dt=1e-3),
+                         ("decaying", 9, 6.0), [("steps", 10, 1e-3), ("w_hat",), ("meas",)]),
         # adaptive CFL step with the reference's row-index quirk
         "cfl32": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9, dt=1e-3),
                   ("decaying", 6, 4.0), [("cfl", 1e-3), ("steps", 5, 2e-3), ("cfl", 2e-3), ("w_hat",)]),
