@@ -44,6 +44,13 @@ static void ns2d_compat_check(ns2d_status s, const char* what) {
     exit(1);
 }
 
+/* Forcings whose values the reference draws on the host each step (STOC,
+   STOC_GAUSS, CONST_GAUSS: force.c:104-433, 540-577). */
+static int ns2d_compat_listed_forcing(void) {
+    return !strcmp(sys_vars->forcing, "STOC") || !strcmp(sys_vars->forcing, "STOC_GAUSS") ||
+           !strcmp(sys_vars->forcing, "CONST_GAUSS");
+}
+
 /* Handle built from sys_vars (filled by GetCMLArgs, utils.c:51-460) and the
    compile-time switches of data_types.h. */
 static ns2d_handle* ns2d_compat_handle(void) {
@@ -69,8 +76,10 @@ static ns2d_handle* ns2d_compat_handle(void) {
 #endif
     if (!strcmp(sys_vars->forcing, "KOLM")) {
         p.forcing = NS2D_FORCING_KOLM;
-    } else if (!strcmp(sys_vars->forcing, "NONE")) {
-        p.forcing = NS2D_FORCING_NONE;
+    } else if (!strcmp(sys_vars->forcing, "ZERO")) {
+        p.forcing = NS2D_FORCING_ZERO;
+    } else if (!strcmp(sys_vars->forcing, "NONE") || ns2d_compat_listed_forcing()) {
+        p.forcing = NS2D_FORCING_NONE;  /* listed-mode forcing goes in by ns2d_set_forcing_modes */
     } else {
         fprintf(stderr, "\n[ERROR] ns2d: forcing \"%s\" is not on the GPU path\n-->> Exiting!\n", sys_vars->forcing);
         exit(1);
@@ -93,6 +102,14 @@ static ns2d_handle* ns2d_compat_handle(void) {
     return g_ns2d;
 }
 
+/* The current run_data->forcing values of a listed-mode forcing, to the GPU. */
+static void ns2d_compat_sync_forcing(ns2d_handle* h) {
+    if (!ns2d_compat_listed_forcing() || !sys_vars->local_forcing_proc) return;
+    ns2d_compat_check(ns2d_set_forcing_modes(h, (int32_t)sys_vars->num_forced_modes, run_data->forcing_indx,
+                                             (const double*)run_data->forcing),
+                      "forcing");
+}
+
 /* RK4Step (solver.c:625): one step of run_data->w_hat, in place.  The host
    side effects of the replaced body are kept: the forcing values of this step
    (ComputeForcing, solver.c:650), which ComputeSystemMeasurables reads, and
@@ -104,6 +121,7 @@ void RK4Step(const double dt, const long int* N, const ptrdiff_t local_Nx, Int_d
     (void)Int_data;
     ns2d_handle* h = ns2d_compat_handle();
     ComputeForcing(dt);
+    ns2d_compat_sync_forcing(h);
     ns2d_compat_check(ns2d_rk4_step_host(h, (double*)run_data->w_hat, dt), "RK4Step");
 #if !defined(__EULER)
     if (sys_vars->EKMN_DRAG_FLAG != EKMN_DRAG) sys_vars->HYPER_VISC_FLAG = HYPER_VISC;
@@ -136,6 +154,7 @@ void NonlinearRHSBatch(fftw_complex* w_hat, fftw_complex* dw_hat_dt, double* non
     (void)w;
     ns2d_handle* h = ns2d_compat_handle();
     const long int N[2] = {sys_vars->N[0], sys_vars->N[1]};
+    ns2d_compat_sync_forcing(h);
     ns2d_compat_check(ns2d_nonlinear_rhs(h, (const double*)w_hat, (double*)dw_hat_dt), "NonlinearRHSBatch");
     ForceConjugacy(w_hat, N);
 }

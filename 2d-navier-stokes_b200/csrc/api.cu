@@ -3,6 +3,7 @@
 // reference function it replaces (EndCar808/2D-Navier-Stokes, Solver/src).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -88,6 +89,7 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.inv_nxny = norm_fac;
     a.status = h->dstatus;
     a.final_tail = 1;
+    a.force_field = h->ffield_on ? (const C*)h->ffield : nullptr;
     a.ntiles = (h->nyf + col_tc(h->nx) - 1) / col_tc(h->nx);
     a.lin = make_lin(h, branch);
 }
@@ -508,6 +510,9 @@ void free_all(ns2d_handle* h) {
         if (p) cudaFree(p);
     for (void* p : h->dp)
         if (p) cudaFree(p);
+    void* fp[] = {h->ffield, h->fidx, h->fval};
+    for (void* p : fp)
+        if (p) cudaFree(p);
     if (h->dp_kptr) cudaFree((void*)h->dp_kptr);
 }
 
@@ -729,6 +734,7 @@ ns2d_status measurables_impl(ns2d_handle* h, ns2d_measures* out, double* spectra
     d.fre = h->fre;
     d.fim = h->fim;
     d.has_force = h->forced ? 1 : 0;
+    d.ffield = h->ffield_on ? (const C*)h->ffield : nullptr;
     d.n_spect = ns;
     d.out = h->ddiag;
     const size_t smem = sizeof(double) * (8 * (size_t)ns + DG_N * 8);
@@ -1183,6 +1189,45 @@ ns2d_status ns2d_step_async(ns2d_handle* h, int32_t nsteps, double dt) {
         }
         if (s) return s;
     }
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_set_forcing_modes(ns2d_handle* h, int32_t n, const int32_t* idx, const double* values) {
+    if (!h || n < 0 || (n > 0 && (!idx || !values))) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    const bool was_on = h->ffield_on;
+    if (n == 0) {
+        h->ffield_on = false;
+        if (was_on) drop_graph(h);
+        return NS2D_OK;
+    }
+    const int64_t total = (int64_t)h->nx * h->nyf;
+    for (int32_t m = 0; m < n; ++m)
+        if (idx[m] < 0 || idx[m] >= total) return fail(h, NS2D_ERR_INVALID, "forcing index outside the half spectrum");
+    if (!h->ffield) CK(h, cudaMalloc(&h->ffield, h->field_bytes));
+    if (h->fcap < n) {
+        if (h->fidx) cudaFree(h->fidx);
+        if (h->fval) cudaFree(h->fval);
+        h->fidx = nullptr;
+        h->fval = nullptr;
+        h->fcap = 0;
+        CK(h, cudaMalloc((void**)&h->fidx, sizeof(int32_t) * n));
+        CK(h, cudaMalloc((void**)&h->fval, sizeof(double2) * n));
+        h->fcap = n;
+    }
+    CK(h, cudaMemsetAsync(h->ffield, 0, h->field_bytes, h->stream));
+    CK(h, cudaMemcpyAsync(h->fidx, idx, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->fval, values, sizeof(double2) * n, cudaMemcpyHostToDevice, h->stream));
+    const int blocks = std::min(148, (n + 255) / 256);
+    if (h->fp32)
+        scatter_forcing_kernel<float><<<blocks, 256, 0, h->stream>>>((float2*)h->ffield, h->nyf, h->ldc, h->fidx, h->fval, n);
+    else
+        scatter_forcing_kernel<double><<<blocks, 256, 0, h->stream>>>((double2*)h->ffield, h->nyf, h->ldc, h->fidx, h->fval, n);
+    h->launches++;
+    CKL(h);
+    CK(h, cudaStreamSynchronize(h->stream));  // the caller's arrays may go away on return
+    h->ffield_on = true;
+    if (!was_on) drop_graph(h);  // captured steps carry the field pointer only when it is on
     return NS2D_OK;
 }
 

@@ -251,6 +251,18 @@ __global__ void zero_modes_kernel(typename Cx<Real>::T* state, int nx, int nyf, 
     }
 }
 
+// Forcing of listed modes: value m goes to flat index idx[m] of the
+// reference layout [nx][nyf] (run_data->forcing_indx), other modes stay 0.
+template <typename Real>
+__global__ void scatter_forcing_kernel(typename Cx<Real>::T* field, int nyf, int ldc, const int32_t* idx,
+                                       const double2* val, int n) {
+    using C = typename Cx<Real>::T;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const int q = idx[m];
+        field[(size_t)(q / nyf) * ldc + (q % nyf)] = cmake<C>((decltype(C::x))val[m].x, (decltype(C::x))val[m].y);
+    }
+}
+
 // Dormand-Prince 5(4) (RK5DPStep, Solver/src/solver.c:360-570, corrected).
 struct DpCoef {
     double c[7];

@@ -21,6 +21,7 @@ struct DiagArgs {
     int force_i, force_j;
     double fre, fim;
     int has_force;
+    const C* ffield;  // forcing of listed modes ([nx][ldc]), may be null
     int n_spect;
     double* out;     // [DG_N] raw totals, then 8 * n_spect raw spectra (zeroed by the host)
 };
@@ -62,6 +63,11 @@ __global__ void __launch_bounds__(256) diag_kernel(DiagArgs<Real> a) {
                 r.x = (Real)((double)r.x - a.fre);
                 r.y = (Real)((double)r.y - a.fim);
             }
+            if (a.ffield) {
+                const C f = a.ffield[(size_t)i * a.ldc + j];
+                r.x = (Real)((double)r.x - (double)f.x);
+                r.y = (Real)((double)r.y - (double)f.y);
+            }
             // creal(w conj(r) + conj(w) r) = 2 Re(w conj r)
             deriv = (wr * (double)r.x + wi * (double)r.y) + ((double)r.x * wr + (double)r.y * wi);
         }
@@ -84,6 +90,12 @@ __global__ void __launch_bounds__(256) diag_kernel(DiagArgs<Real> a) {
         if (a.has_force && i == a.force_i && j == a.force_j) {
             // cabs(forcing * w_hat[forced])  (sys_msr.c:135-139)
             const double pr = a.fre * wr - a.fim * wi, pi = a.fre * wi + a.fim * wr;
+            acc[DG_FORC] += sqrt(pr * pr + pi * pi);
+        }
+        if (a.ffield) {
+            const C f = a.ffield[(size_t)i * a.ldc + j];
+            const double fr = (double)f.x, fi = (double)f.y;
+            const double pr = fr * wr - fi * wi, pi = fr * wi + fi * wr;
             acc[DG_FORC] += sqrt(pr * pr + pi * pi);
         }
         const int b = (int)round(sqrt(k_sqr));

@@ -63,6 +63,12 @@ struct ns2d_handle {
     // adjoint's own buffers (adjoint.cu)
     void* cap_step = nullptr;
     ns2d::AdjointState* adj = nullptr;
+    // forcing of listed modes (ns2d_set_forcing_modes): dense field added to the RHS
+    void* ffield = nullptr;
+    bool ffield_on = false;
+    int32_t* fidx = nullptr;
+    double2* fval = nullptr;
+    int fcap = 0;
     // Dormand-Prince stages k0..k6, y0 and the stage input (allocated on first use)
     void* dp[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     const void** dp_kptr = nullptr;  // device array of the seven stage pointers

@@ -100,6 +100,7 @@ struct ColArgs {
     int lin_stage;       // 0 none, 1: rhs += dt D X (quirk), 2: rhs -= D X (corrected)
     LinOp lin;
     const double2* cn;   // COL_FINAL, CN schemes: per-mode ((2-D)/(2+D), 2dt/(2+D)), stride ldc
+    const C* force_field;  // forcing added to every mode of the RHS ([nx][ldc]), may be null
     double inv_nxny;     // 1/(Nx Ny)
     int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
     int ntiles;          // number of column tiles of this field
@@ -320,6 +321,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             }
             // forcing (solver.c:1022-1027)
             if (a.has_force && i == a.force_i && ky == a.force_j) r = cadd(r, a.force_val);
+            if (a.force_field) r = cadd(r, a.force_field[(size_t)i * ldc + kyc]);
             if constexpr (MODE == COL_RHS) {
                 // stage derivative with the explicit linear term (Dormand-Prince
                 // stages): r -= bracket(|k|^2) X, X the RHS input

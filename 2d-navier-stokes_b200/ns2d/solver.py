@@ -94,6 +94,15 @@ class Solver:
     def ab4_step(self, dt, iters):
         self._ck(self.L.ns2d_ab4_step(self.h, dt, iters))
 
+    def set_forcing_modes(self, idx, values):
+        """Forcing of listed modes (flat indices into [nx][ny/2+1], complex
+        values), added to every RHS until changed; empty removes it."""
+        idx = np.ascontiguousarray(idx, np.int32)
+        values = np.ascontiguousarray(values, np.complex128)
+        assert idx.shape == values.shape
+        self._ck(self.L.ns2d_set_forcing_modes(self.h, len(idx), idx.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               _ptr(values.view(np.float64)) if len(idx) else None))
+
     def dp5_step(self, dt):
         """One Dormand-Prince 5(4) trial step (RK5DPStep, corrected); returns
         the scaled error estimate."""

@@ -138,6 +138,14 @@ ns2d_status ns2d_get_w_hat_device(ns2d_handle* h, double* d_w_hat);
 
 /* ComputeForcing (Solver/src/force.c:516): forcing values for this step. */
 ns2d_status ns2d_compute_forcing(ns2d_handle* h, double dt);
+/* Forcing of listed modes, added to every RHS evaluation until changed (the
+   reference's run_data->forcing / forcing_indx, added at solver.c:1022-1027):
+   values[2m], values[2m+1] = re, im of the forcing at flat index idx[m] of the
+   [nx][ny/2+1] half spectrum.  The stochastic and Gaussian forcings of
+   force.c:104-433 draw their values with glibc rand() on the host each step
+   (ComputeForcing); a caller passes them here.  n = 0 removes the forcing.
+   Adds to the built-in KOLM forcing when both are set. */
+ns2d_status ns2d_set_forcing_modes(ns2d_handle* h, int32_t n, const int32_t* idx, const double* values);
 
 /* NonlinearRHSBatch (Solver/src/solver.c:884; solver.h:39).  in == NULL means
    the state itself (stage-1 form).  out receives the dealiased nonlinear term

@@ -285,7 +285,7 @@ class RefSolver:
         return s, sp.reshape(8, self.n_spect)
 
 
-def solve(params, variant="rk4cn", u0="TG_VORT", T=0.05, save_every=10, threads=1):
+def solve(params, variant="rk4cn", u0="TG_VORT", T=0.05, save_every=10, threads=1, forcing=None):
     """Run SpectralSolve (Solver/src/solver.c:54-251) of a reference library
     from the initial condition u0 over [0, T]; returns (w_hat at the last save,
     its time, number of saves).  The library keeps global state: call once per
@@ -297,7 +297,7 @@ def solve(params, variant="rk4cn", u0="TG_VORT", T=0.05, save_every=10, threads=
     L.ref_solve.argtypes = [C.c_void_p, C.c_int]
     L.ref_saved_w_hat.argtypes = [_dp, _dp]
     L.ref_saved_w_hat.restype = C.c_long
-    forcing = {0: b"NONE", 1: b"KOLM", 2: b"ZERO"}[params.forcing]
+    forcing = forcing.encode() if forcing else {0: b"NONE", 1: b"KOLM", 2: b"ZERO"}[params.forcing]
     rp = _RefParams(nx=params.nx, ny=params.ny, nu=params.nu, hyper_visc_flag=params.hyper_visc_flag,
                     hyper_visc_pow=params.hyper_visc_pow, ekmn_alpha=params.ekmn_alpha,
                     ekmn_drag_flag=params.ekmn_drag_flag, ekmn_drag_pow=params.ekmn_drag_pow,

@@ -32,10 +32,10 @@ def _program_worker(name, q):
     q.put(make_golden.run_program(ref, w0, program, True))
 
 
-def _solve_worker(variant, kw, u0, T, every, q):
+def _solve_worker(variant, kw, u0, T, every, forcing, q):
     import pyoracle
     from ns2d import abi
-    q.put(pyoracle.solve(abi.default_params(**kw), variant, u0, T=T, save_every=every))
+    q.put(pyoracle.solve(abi.default_params(**kw), variant, u0, T=T, save_every=every, forcing=forcing))
 
 
 def _spawn(target, *args):
@@ -69,18 +69,23 @@ def test_reference_harness_on_gpu_entry_points(name):
 
 
 @needs_dropin
-@pytest.mark.parametrize("u0,kw,T,every", [
-    ("TG_VORT", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, ekmn_drag_flag=1), 0.05, 10),
-    ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3), 0.05, 10),
+@pytest.mark.parametrize("u0,kw,T,every,forcing", [
+    ("TG_VORT", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, ekmn_drag_flag=1), 0.05, 10, None),
+    ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3), 0.05, 10, None),
     ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9),
-     0.5, 1),
+     0.5, 1, None),
+    # the reference's stochastic forcings draw their values with rand() on the
+    # host; the drop-in passes them to the GPU every step
+    ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, force_k=4, force_scale=1.0), 0.03, 10, "STOC"),
+    ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, force_k=4, force_scale=1.0), 0.03, 10, "STOC_GAUSS"),
+    ("DECAY_TURB_BB", dict(nx=64, ny=64, nu=1e-3, dt=1e-3, force_k=2), 0.03, 10, "ZERO"),
 ])
-def test_spectral_solve_on_gpu_entry_points(u0, kw, T, every):
-    """The reference's own SpectralSolve loop (initial condition, steps, saves,
-    measurables, adaptive dt, SystemCheck): the state it saves last agrees
-    between the CPU build and the drop-in build to 1e-12."""
-    w_cpu, t_cpu, n_cpu = _spawn(_solve_worker, "rk4cn", kw, u0, T, every)
-    w_gpu, t_gpu, n_gpu = _spawn(_solve_worker, "dropin", kw, u0, T, every)
+def test_spectral_solve_on_gpu_entry_points(u0, kw, T, every, forcing):
+    """The reference's own SpectralSolve loop (initial condition, forcing,
+    steps, saves, measurables, adaptive dt, SystemCheck): the state it saves
+    last agrees between the CPU build and the drop-in build to 1e-12."""
+    w_cpu, t_cpu, n_cpu = _spawn(_solve_worker, "rk4cn", kw, u0, T, every, forcing)
+    w_gpu, t_gpu, n_gpu = _spawn(_solve_worker, "dropin", kw, u0, T, every, forcing)
     assert n_gpu == n_cpu and n_cpu >= 2
     assert abs(t_gpu - t_cpu) <= 1e-12 * max(t_cpu, 1.0)
     assert rel_err(w_gpu, w_cpu) <= 1e-12
