@@ -407,7 +407,7 @@ ns2d_status dp5_step_impl(ns2d_handle* h, double dt, double* err) {
 // pass with a reduction or a store.
 template <typename Real>
 ns2d_status c2r_impl(ns2d_handle* h, const InvField<Real>* fields, int nf, int op, double* outA, double* outB,
-                     double* result) {
+                     double* result, double scale = 0.0) {
     using C = Cplx<Real>;
     InvArgs<Real> ia;
     std::memset(&ia, 0, sizeof(ia));
@@ -427,7 +427,7 @@ ns2d_status c2r_impl(ns2d_handle* h, const InvField<Real>* fields, int nf, int o
     ra.B = nf > 1 ? (const C*)h->f[1] : nullptr;
     ra.ldc = h->ldc;
     ra.tw = (const C*)h->tw;
-    ra.scale = 1.0 / (double)(h->nx * h->ny);
+    ra.scale = scale != 0.0 ? scale : 1.0 / (double)(h->nx * h->ny);
     ra.dx = 2.0 * M_PI / (double)h->nx;
     ra.dy = 2.0 * M_PI / (double)h->ny;
     ra.maxbits = h->dmax;
@@ -664,6 +664,51 @@ ns2d_status state_to_host(ns2d_handle* h, const void* src, double* host) {
     if (s) return s;
     CK(h, cudaMemcpyAsync(host, h->dio, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
+    return NS2D_OK;
+}
+
+// Unnormalised r2c of a host [nx][ny] real field to a host half spectrum.
+template <typename Real>
+ns2d_status r2c_host_impl(ns2d_handle* h, const double* real, double* spec) {
+    using C = Cplx<Real>;
+    CK(h, cudaMemcpyAsync(h->dreal, real, sizeof(double) * (size_t)h->nx * h->ny, cudaMemcpyHostToDevice, h->stream));
+    with_size<Real>(h->nx, [&](auto L) {
+        decltype(L)::fwd(FWD_ROWS, h->dreal, nullptr, (C*)h->f[0], h->nx, h->ldc, (const C*)h->tw, h->stream);
+        decltype(L)::fwd(FWD_COLS, nullptr, (const C*)h->f[0], (C*)h->f[1], h->nyf, h->ldc, (const C*)h->tw,
+                         h->stream);
+    });
+    h->launches += 2;
+    CKL(h);
+    return state_to_host(h, h->f[1], spec);
+}
+
+// Unnormalised c2r of a host half spectrum to a host [nx][ny] real field.
+template <typename Real>
+ns2d_status c2r_host_impl(ns2d_handle* h, const double* spec, double* real) {
+    ns2d_status s = host_to_state(h, spec, h->f[2]);
+    if (s) return s;
+    InvField<Real> f[1];
+    std::memset(f, 0, sizeof(f));
+    f[0].p = (const Cplx<Real>*)h->f[2];
+    f[0].rs = h->ldc;
+    f[0].es = 1;
+    if ((s = c2r_impl<Real>(h, f, 1, R2_STORE, h->dreal, nullptr, nullptr, 1.0))) return s;
+    CK(h, cudaMemcpyAsync(real, h->dreal, sizeof(double) * (size_t)h->nx * h->ny, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return NS2D_OK;
+}
+
+template <typename Real>
+ns2d_status mean_flow_impl(ns2d_handle* h, double* mean_x, double* mean_y) {
+    mean_flow_kernel<Real><<<h->nx + h->nyf, 256, 0, h->stream>>>((const Cplx<Real>*)h->state, h->nx, h->nyf, h->ldc,
+                                                                h->dpart);
+    h->launches++;
+    CKL(h);
+    std::vector<double> buf((size_t)h->nx + h->nyf);
+    CK(h, cudaMemcpyAsync(buf.data(), h->dpart, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (mean_y) std::memcpy(mean_y, buf.data(), sizeof(double) * h->nx);
+    if (mean_x) std::memcpy(mean_x, buf.data() + h->nx, sizeof(double) * h->nyf);
     return NS2D_OK;
 }
 
@@ -1157,6 +1202,25 @@ ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w) {
     CK(h, cudaMemcpyAsync(w, h->dreal, sizeof(double) * (size_t)h->nx * h->ny, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     return NS2D_OK;
+}
+
+ns2d_status ns2d_fft_r2c(ns2d_handle* h, const double* real, double* spec) {
+    if (!h || !real || !spec) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    return DISPATCH(h, r2c_host_impl, h, real, spec);
+}
+
+ns2d_status ns2d_fft_c2r(ns2d_handle* h, const double* spec, double* real) {
+    if (!h || !spec || !real) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    return DISPATCH(h, c2r_host_impl, h, spec, real);
+}
+
+ns2d_status ns2d_mean_flow(ns2d_handle* h, double* mean_x, double* mean_y) {
+    if (!h || (!mean_x && !mean_y)) return NS2D_ERR_INVALID;
+    if ((size_t)h->nx + h->nyf > 4096) return fail(h, NS2D_ERR_UNSUPPORTED, "mean flow needs nx + ny/2 + 1 <= 4096");
+    cudaSetDevice(h->p.device);
+    return DISPATCH(h, mean_flow_impl, h, mean_x, mean_y);
 }
 
 ns2d_status ns2d_rk4_step_host(ns2d_handle* h, double* w_hat, double dt) {

@@ -204,6 +204,95 @@ __global__ void unpack_kernel(const typename Cx<Real>::T* __restrict__ src, doub
     }
 }
 
+// Forward (e^{-i...}) unnormalised transform passes of a real field, the r2c
+// of FFTW's fftw_mpi_plan_dft_r2c_2d that the reference applies to real-space
+// initial conditions (Solver/src/solver.c:1178, 1200, 1833, 1873).
+//   ROWS: block = TC rows, one transform per row: real in[x][y] (double,
+//         [nx][ny]) -> row spectrum out[x][ky] for ky <= ny/2 ([nx][ldc]).
+//   COLS: block = TC columns: out[i][ky] = sum_x in[x][ky] e^{-2 pi i x kx / nx}.
+// Used at set-up only (initial conditions, file input), so rows are read
+// with the columns' interleaved smem layout instead of a packed real transform.
+enum FwdPass : int { FWD_ROWS = 0, FWD_COLS = 1 };
+
+template <typename Real, int N, int TC, int PASS>
+__global__ void __launch_bounds__(Plan<N>::T * TC) fwd_kernel(const double* __restrict__ real_in,
+                                                              const typename Cx<Real>::T* __restrict__ in,
+                                                              typename Cx<Real>::T* __restrict__ out, int nlines,
+                                                              int ldc, const typename Cx<Real>::T* __restrict__ tw) {
+    using C = typename Cx<Real>::T;
+    constexpr int T = Plan<N>::T;
+    constexpr int E = N / T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int c = threadIdx.x % TC;
+    const int t = threadIdx.x / TC;
+    const int line = blockIdx.x * TC + c;
+    const bool valid = line < nlines;
+    const int lc = valid ? line : 0;
+    const TwSeed<C> seed = twiddle_seeds<N>(tw, t);
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int e = t + T * m;
+        if constexpr (PASS == FWD_ROWS) {
+            v[m] = cmake<C>(valid ? (Real)real_in[(size_t)lc * N + e] : (Real)0, (Real)0);
+        } else {
+            v[m] = valid ? in[(size_t)e * ldc + lc] : cmake<C>(0, 0);
+        }
+    }
+    fft<N, -1, TC>(v, sm, seed, t, c);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int e = t + T * m;
+            if constexpr (PASS == FWD_ROWS) {
+                if (e <= N / 2) out[(size_t)lc * ldc + e] = v[m];
+            } else {
+                out[(size_t)e * ldc + lc] = v[m];
+            }
+        }
+    }
+}
+
+// Mean-flow sums of ComputeSystemMeasurables for one call: for every row
+// kx, mean_y = sum_ky c_ky |v_hat| (Solver/src/sys_msr.c:199, 227), and for
+// every column ky, mean_x = sum_kx c_ky |u_hat|, with u_hat = i ky w/k^2,
+// v_hat = -i kx w/k^2, c = 1 on the ky = 0 and ky = ny/2 columns and 2
+// elsewhere, the (0,0) mode skipped.  Blocks [0, nx) reduce rows, blocks
+// [nx, nx + nyf) columns; out = [mean_y (nx) | mean_x (nyf)].  The column sum
+// is what sys_msr.c:338-348 intends: that loop indexes the ky array with the
+// row counter and reuses the last k^2 of the previous loop.
+template <typename Real>
+__global__ void __launch_bounds__(256) mean_flow_kernel(const typename Cx<Real>::T* __restrict__ w, int nx, int nyf,
+                                                        int ldc, double* __restrict__ out) {
+    __shared__ double red[8];
+    const bool row = blockIdx.x < (unsigned)nx;
+    const int line = row ? blockIdx.x : blockIdx.x - nx;
+    const int count = row ? nyf : nx;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < count; q += blockDim.x) {
+        const int i = row ? line : q;
+        const int ky = row ? q : line;
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        if (kx == 0 && ky == 0) continue;
+        const double k2 = (double)kx * kx + (double)ky * ky;
+        const auto z = w[(size_t)i * ldc + ky];
+        const double wr = (double)z.x, wi = (double)z.y;
+        const double kk = row ? (double)kx : (double)ky;
+        const double a = hypot(kk * wi / k2, kk * wr / k2);
+        acc += (ky == 0 || ky == nyf - 1) ? a : 2.0 * a;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+        out[blockIdx.x] = s;
+    }
+}
+
 // ApplyDealiasing (Solver/src/solver.c:1039-1099) on `dim` interleaved fields
 // in the reference layout.
 template <typename Real>

@@ -48,6 +48,8 @@ struct Launch {
         set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, c2r_smem());
         set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_CFL>, c2r_smem());
         set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_STORE>, c2r_smem());
+        set((const void*)fwd_kernel<Real, N, S::TC, FWD_ROWS>, inv_smem());
+        set((const void*)fwd_kernel<Real, N, S::TC, FWD_COLS>, inv_smem());
         return e;
     }
 
@@ -67,6 +69,15 @@ struct Launch {
     static void col_inv(const InvArgs<Real>& a, cudaStream_t s) {
         dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
         col_inv_kernel<Real, N, S::TC><<<grid, block, inv_smem(), s>>>(a);
+    }
+    // Forward transform passes (set-up only): rows of a real [N][N] field, then columns.
+    static void fwd(int pass, const double* real_in, const C* in, C* out, int nlines, int ldc, const C* tw,
+                    cudaStream_t s) {
+        dim3 grid((nlines + S::TC - 1) / S::TC), block(S::T * S::TC);
+        if (pass == FWD_ROWS)
+            fwd_kernel<Real, N, S::TC, FWD_ROWS><<<grid, block, inv_smem(), s>>>(real_in, in, out, nlines, ldc, tw);
+        else
+            fwd_kernel<Real, N, S::TC, FWD_COLS><<<grid, block, inv_smem(), s>>>(real_in, in, out, nlines, ldc, tw);
     }
     static void row_c2r(int op, const RowC2RArgs<Real>& a, cudaStream_t s) {
         dim3 grid(N / (2 * S::PAIRS)), block(S::T * 2 * S::PAIRS);

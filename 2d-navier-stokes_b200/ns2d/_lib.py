@@ -53,6 +53,9 @@ def load():
         "ns2d_system_check": (C.c_int, [H, C.c_double, C.c_int64]),
         "ns2d_system_measurables": (C.c_int, [H, C.POINTER(abi.Measures), _dp]),
         "ns2d_get_w_real": (C.c_int, [H, _dp]),
+        "ns2d_fft_r2c": (C.c_int, [H, _dp, _dp]),
+        "ns2d_fft_c2r": (C.c_int, [H, _dp, _dp]),
+        "ns2d_mean_flow": (C.c_int, [H, _dp, _dp]),
         "ns2d_set_stream": (C.c_int, [H, C.c_void_p]),
         "ns2d_synchronize": (C.c_int, [H]),
         "ns2d_launch_count": (C.c_int64, [H]),

@@ -75,6 +75,29 @@ class Solver:
         self._ck(self.L.ns2d_get_w_real(self.h, _ptr(w)))
         return w
 
+    def fft_r2c(self, real):
+        """Unnormalised r2c of a real [nx][ny] field (FFTW conventions)."""
+        real = np.ascontiguousarray(real, dtype=np.float64)
+        assert real.shape == (self.nx, self.ny)
+        out = np.zeros((self.nx, self.ny // 2 + 1), dtype=np.complex128)
+        self._ck(self.L.ns2d_fft_r2c(self.h, _ptr(real), _ptr(out)))
+        return out
+
+    def fft_c2r(self, spec):
+        """Unnormalised c2r of a half spectrum [nx][ny/2+1] (FFTW conventions)."""
+        spec = np.ascontiguousarray(spec, dtype=np.complex128)
+        assert spec.shape == (self.nx, self.ny // 2 + 1)
+        out = np.zeros((self.nx, self.ny))
+        self._ck(self.L.ns2d_fft_c2r(self.h, _ptr(spec), _ptr(out)))
+        return out
+
+    def mean_flow(self):
+        """(mean_x [ny/2+1], mean_y [nx]) sums of one measurables call."""
+        mx = np.zeros(self.ny // 2 + 1)
+        my = np.zeros(self.nx)
+        self._ck(self.L.ns2d_mean_flow(self.h, _ptr(mx), _ptr(my)))
+        return mx, my
+
     # reference entry points
     def compute_forcing(self, dt):
         self._ck(self.L.ns2d_compute_forcing(self.h, dt))

@@ -217,6 +217,23 @@ ns2d_status ns2d_system_measurables(ns2d_handle* h, ns2d_measures* out, double* 
 /* Real-space vorticity [nx][ny] (c2r of the state, normalised). */
 ns2d_status ns2d_get_w_real(ns2d_handle* h, double* w);
 
+/* The reference's 2-D FFTW transforms on the handle's device and precision,
+   host buffers, unnormalised (fftw_mpi_plan_dft_r2c_2d / _c2r_2d,
+   Solver/src/solver.c:2603-2615): r2c maps a real [nx][ny] field to the half
+   spectrum [nx][ny/2+1] complex128 (e^{-i..}); c2r maps back (e^{+i..}) and,
+   like FFTW's c2r, reads only the real parts of the ky = 0 and ky = ny/2
+   columns.  For initial conditions and file input (solver.c:1139-1873);
+   they use the handle's scratch fields, not its state. */
+ns2d_status ns2d_fft_r2c(ns2d_handle* h, const double* real, double* spec);
+ns2d_status ns2d_fft_c2r(ns2d_handle* h, const double* spec, double* real);
+
+/* Mean-flow sums of one ComputeSystemMeasurables call on the state:
+   mean_y[kx row] = sum_ky c |v_hat| (Solver/src/sys_msr.c:199, 227) and
+   mean_x[ky] = sum_kx c |u_hat|, c = 1 on ky = 0, ny/2 and 2 elsewhere.
+   mean_x is the sum sys_msr.c:338-348 intends (that loop reads the ky array
+   with the row counter).  Either pointer may be NULL; needs nx + ny/2 + 1 <= 4096. */
+ns2d_status ns2d_mean_flow(ns2d_handle* h, double* mean_x, double* mean_y);
+
 /* The nonlinear term of NonlinearRHSBatch for callers that cannot allocate
    device memory.  No counterpart in the reference; it exists for code that runs
    under somebody else's stream capture (cudaMalloc cannot be recorded into a
