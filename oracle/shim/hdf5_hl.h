@@ -2,5 +2,6 @@
 #ifndef NS2D_SHIM_HDF5_HL_H
 #define NS2D_SHIM_HDF5_HL_H
 #include "hdf5.h"
-static inline herr_t H5LTread_dataset_double(hid_t f, const char* n, double* d) { (void)f; (void)n; (void)d; return -1; }
+herr_t H5LTmake_dataset(hid_t loc, const char* name, int rank, const hsize_t* dims, hid_t type, const void* buf);
+herr_t H5LTread_dataset_double(hid_t loc, const char* name, double* buf);
 #endif

@@ -1,7 +1,7 @@
 /*
- * oracle/shim/shim.c -- bodies for the single-rank FFTW3-MPI stand-in and the
- * no-op output hooks that the reference solver calls (test infrastructure
- * only).  Transforms are oracle/fft.c.  fftw_malloc returns zeroed memory so
+ * oracle/shim/shim.c -- bodies for the single-rank FFTW3-MPI stand-in (test
+ * infrastructure only); the no-op output hooks are in hooks.c.  Transforms are
+ * oracle/fft.c.  fftw_malloc returns zeroed memory so
  * that reference arrays it never initialises (e.g. the mean-flow sums in
  * Solver/src/sys_msr.c:454-461) are deterministic.
  */
@@ -75,22 +75,3 @@ void fftw_mpi_execute_dft_c2r(const fftw_plan p, fftw_complex* in, double* out) 
     offt_c2r_2d(p->nx, p->ny, p->howmany, in, out);
 }
 void fftw_destroy_plan(fftw_plan p) { free(p); }
-
-/* Output hooks of Solver/src/hdf5_funcs.h and utils.h: no file I/O here. */
-void CreateOutputFilesWriteICs(const long int* N, double dt) { (void)N; (void)dt; }
-/* A harness may watch the saves (e.g. to keep the state SpectralSolve saves). */
-void (*shim_write_hook)(double t, long int iters) = 0;
-void WriteDataToFile(double t, double dt, long int iters) {
-    (void)dt;
-    if (shim_write_hook) shim_write_hook(t, iters);
-}
-void FinalWriteAndCloseOutputFiles(const long int* N, int iters, int save_data_indx) {
-    (void)N; (void)iters; (void)save_data_indx;
-}
-void OpenTestingFile(void) {}
-void WriteTestDataReal(double* data, char* dset_name, int dset_rank, int* dset_dims, int local_dim_x) {
-    (void)data; (void)dset_name; (void)dset_rank; (void)dset_dims; (void)local_dim_x;
-}
-void WriteTestDataFourier(fftw_complex* data, char* dset_name, int dim_x, int dim_y, int local_dim_x) {
-    (void)data; (void)dset_name; (void)dim_x; (void)dim_y; (void)local_dim_x;
-}
