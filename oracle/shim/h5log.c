@@ -103,6 +103,9 @@ hid_t H5Fcreate(const char* name, unsigned flags, hid_t fcpl, hid_t fapl) {
     }
     snprintf(f->path, sizeof(f->path), "%s", name);
     fwrite("NS2DLOG1", 1, 8, f->fp);
+    /* on disk now: with transient iterations the reference never closes this
+       handle (hdf5_funcs.c:400-410) and reopens the file to append */
+    fflush(f->fp);
     for (int i = 0; i < g_ngroups; ++i)
         if (!strcmp(g_groups[i].file, name)) g_groups[i].file[0] = '\0';
     return id;
