@@ -229,7 +229,7 @@ AdjColArgs<Real> col_common(ns2d_handle* h) {
     a.nyf = h->nyf;
     a.norm2 = (Real)std::pow(1.0 / (double)(h->nx * h->ny), 2.0);
     const int m = (int)(h->nx / 3.0);
-    a.kmax_sqr = m * m;
+    a.kmax_sqr = m * m + h->p.dealias_edge;
     a.dealias = h->p.dealias;
     a.houli_int = (h->p.quirks & NS2D_QUIRK_HOU_LI_INT) ? 1 : 0;
     a.kolm = (h->p.forcing == NS2D_FORCING_KOLM) ? 1 : 0;

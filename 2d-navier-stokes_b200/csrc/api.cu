@@ -75,7 +75,7 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.ldc = h->ldc;
     a.nyf = h->nyf;
     const int m = (int)(h->nx / 3.0);
-    a.kmax_sqr = m * m;
+    a.kmax_sqr = m * m + h->p.dealias_edge;
     a.dealias = h->p.dealias;
     a.houli_int = quirk(h, NS2D_QUIRK_HOU_LI_INT) ? 1 : 0;
     a.kolm = (h->p.forcing == NS2D_FORCING_KOLM) ? 1 : 0;
@@ -874,7 +874,8 @@ ns2d_status ns2d_create(const ns2d_params* p, ns2d_handle** out) {
     if (p->nx != p->ny) return NS2D_ERR_UNSUPPORTED;
     if (!is_pow2(p->nx) || p->nx < 16 || p->nx > 2048) return NS2D_ERR_UNSUPPORTED;
     if (p->integrator < 0 || p->integrator > 3 || p->dealias < 0 || p->dealias > 1 || p->forcing < 0 ||
-        p->forcing > 2 || (p->precision != NS2D_FP64 && p->precision != NS2D_FP32))
+        p->forcing > 2 || (p->precision != NS2D_FP64 && p->precision != NS2D_FP32) || p->dealias_edge < 0 ||
+        p->dealias_edge > 1)
         return NS2D_ERR_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NS2D_ERR_NO_DEVICE;
@@ -1075,7 +1076,7 @@ ns2d_status ns2d_apply_dealiasing(ns2d_handle* h, double* arr, int32_t dim) {
     CK(h, cudaMalloc(&d, sizeof(double2) * n));
     CK(h, cudaMemcpy(d, arr, sizeof(double2) * n, cudaMemcpyHostToDevice));
     const int m = (int)(h->nx / 3.0);
-    dealias_kernel<double><<<296, 256, 0, h->stream>>>(d, dim, h->nx, h->ny, m * m, h->p.dealias,
+    dealias_kernel<double><<<296, 256, 0, h->stream>>>(d, dim, h->nx, h->ny, m * m + h->p.dealias_edge, h->p.dealias,
                                                        quirk(h, NS2D_QUIRK_HOU_LI_INT) ? 1 : 0,
                                                        h->p.forcing == NS2D_FORCING_KOLM ? 1 : 0);
     h->launches++;

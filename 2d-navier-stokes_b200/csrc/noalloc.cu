@@ -129,7 +129,7 @@ extern "C" ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const do
     a.ldc = nyf;
     a.nyf = nyf;
     const int m = (int)(n / 3.0);
-    a.kmax_sqr = m * m;
+    a.kmax_sqr = m * m + (p->dealias_edge ? 1 : 0);
     a.dealias = p->dealias;
     a.houli_int = (p->quirks & NS2D_QUIRK_HOU_LI_INT) ? 1 : 0;
     a.kolm = (p->forcing == NS2D_FORCING_KOLM) ? 1 : 0;

@@ -657,15 +657,20 @@ int ns2d_h5_close(ns2d_h5_file* f) {
 }
 
 /* ---- reading ------------------------------------------------------------------ */
-/* Reader for one dataset of doubles, for initial conditions read from file
-   (MAX_PALIN, Solver/src/solver.c:1775-1853): superblock version 0 or 1 with
+/* Reader for files in libhdf5's default layout, for input files (MAX_PALIN,
+   Solver/src/solver.c:1775-1853) and for post-processing saved runs
+   (PostProcessing/src/hdf5_funcs.c:33-170): superblock version 0 or 1 with
    8-byte offsets and lengths, version-1 object headers (with continuation
-   blocks), symbol-table groups, IEEE little-endian doubles, contiguous or
-   compact layout (message version 3).  This is what libhdf5 and h5py write by
-   default; other layouts are reported as unsupported. */
+   blocks), symbol-table groups, datasets of IEEE little-endian doubles, 32-bit
+   little-endian ints or the {r, i} compound of two doubles, contiguous or
+   compact layout (message version 3), version-1 attributes of one double.
+   Other layouts are reported as unsupported.  Each call opens the file, finds
+   its object and closes it again. */
 typedef struct h5_in {
     FILE* fp;
     uint64_t size;
+    int leaf_k, node_k;
+    uint64_t root_oh;
 } h5_in;
 
 static int rd(h5_in* in, uint64_t addr, void* dst, size_t n) {
@@ -678,6 +683,24 @@ static uint64_t le(const unsigned char* p, int n) {
     uint64_t v = 0;
     for (int i = n - 1; i >= 0; --i) v = (v << 8) | p[i];
     return v;
+}
+
+static int open_in(h5_in* in, const char* path) {
+    memset(in, 0, sizeof(*in));
+    in->fp = fopen(path, "rb");
+    if (!in->fp) return failf(NULL, "cannot open %s: %s", path, strerror(errno));
+    unsigned char sb[56], ent[40];
+    fseeko(in->fp, 0, SEEK_END);
+    in->size = (uint64_t)ftello(in->fp);
+    static const unsigned char sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+    if (rd(in, 0, sb, 56) || memcmp(sb, sig, 8) != 0) return failf(NULL, "%s is not an HDF5 file (superblock at 0 only)", path);
+    if (sb[8] > 1 || sb[13] != 8 || sb[14] != 8)
+        return failf(NULL, "superblock version %d / offset size %d unsupported", sb[8], sb[13]);
+    in->leaf_k = (int)le(sb + 16, 2);
+    in->node_k = (int)le(sb + 18, 2);
+    if (in->leaf_k <= 0 || in->node_k <= 0 || rd(in, sb[8] == 0 ? 56 : 60, ent, 40)) return failf(NULL, "bad superblock");
+    in->root_oh = le(ent + 8, 8);
+    return 0;
 }
 
 /* Messages of the v1 object header at addr: calls fn(ctx, type, body, size). */
@@ -721,16 +744,69 @@ static int walk_header(h5_in* in, uint64_t addr, msg_fn fn, void* ctx) {
     return 0;
 }
 
+/* Element type (NS2D_H5_*) of the datatype message at b, or -1. */
+static int is_ieee_double(const unsigned char* b, size_t n) {
+    return n >= 20 && (b[0] & 0x0f) == 1 && le(b + 4, 4) == 8 && !(b[1] & 1) && le(b + 10, 2) == 64 && b[12] == 52 &&
+           b[13] == 11 && b[15] == 52 && le(b + 16, 4) == 1023;
+}
+static int dtype_code(const unsigned char* b, size_t n) {
+    if (n < 8) return -1;
+    const int cls = b[0] & 0x0f, ver = b[0] >> 4;
+    const uint64_t size = le(b + 4, 4);
+    if (is_ieee_double(b, n)) return NS2D_H5_F64;
+    if (cls == 0 && size == 4 && n >= 12 && !(b[1] & 1) && (b[1] & 8) && le(b + 10, 2) == 32) return NS2D_H5_I32;
+    if (cls == 6 && size == 16 && le(b + 1, 2) == 2 && (ver == 1 || ver == 3)) {
+        size_t p = 8;
+        const char* names[2] = {"r", "i"};
+        for (int m = 0; m < 2; ++m) {
+            const size_t l = strlen(names[m]) + 1;
+            if (p + l > n || memcmp(b + p, names[m], l) != 0) return -1;
+            uint64_t off;
+            if (ver == 1) {
+                p += (l + 7) & ~(size_t)7;
+                if (p + 32 > n) return -1;
+                off = le(b + p, 4);
+                p += 32;
+            } else {
+                p += l;
+                if (p + 1 > n) return -1;
+                off = b[p];
+                p += 1;
+            }
+            if (off != 8u * (unsigned)m || !is_ieee_double(b + p, n - p)) return -1;
+            p += 20;
+        }
+        return NS2D_H5_C128;
+    }
+    return -1;
+}
+
 typedef struct obj_info {
     uint64_t btree, heap;
-    int is_group, has_type, rank;
-    uint64_t count;
-    int dbl_ok;
+    int is_group, type, rank;
+    uint64_t dims[8], count;
     int layout; /* 1 contiguous, 0 compact, -1 none */
     uint64_t data_addr, data_size;
     unsigned char compact[4096];
     size_t compact_size;
+    const char* want_attr; /* attribute wanted, if any */
+    int attr_found;
+    double attr_value;
 } obj_info;
+
+static int dataspace(const unsigned char* b, size_t n, int* rank, uint64_t* dims, uint64_t* count) {
+    if (n < 8) return failf(NULL, "dataspace message unsupported");
+    const int ver = b[0], r = b[1];
+    const size_t at = ver == 1 ? 8 : 4;
+    if ((ver != 1 && ver != 2) || r > 8 || at + 8 * (size_t)r > n) return failf(NULL, "dataspace message unsupported");
+    *rank = r;
+    *count = 1;
+    for (int i = 0; i < r; ++i) {
+        dims[i] = le(b + at + 8 * i, 8);
+        *count *= dims[i];
+    }
+    return 0;
+}
 
 static int info_fn(void* ctx, int type, const unsigned char* b, size_t n) {
     obj_info* o = (obj_info*)ctx;
@@ -738,19 +814,10 @@ static int info_fn(void* ctx, int type, const unsigned char* b, size_t n) {
         o->is_group = 1;
         o->btree = le(b, 8);
         o->heap = le(b + 8, 8);
-    } else if (type == 0x01 && n >= 8) {
-        const int ver = b[0], rank = b[1];
-        const size_t at = ver == 1 ? 8 : 4;
-        if ((ver != 1 && ver != 2) || at + 8 * (size_t)rank > n) return failf(NULL, "dataspace message unsupported");
-        o->rank = rank;
-        o->count = 1;
-        for (int i = 0; i < rank; ++i) o->count *= le(b + at + 8 * i, 8);
-    } else if (type == 0x03 && n >= 20) {
-        o->has_type = 1;
-        const int cls = b[0] & 0x0f;
-        const uint64_t size = le(b + 4, 4);
-        o->dbl_ok = cls == 1 && size == 8 && !(b[1] & 1) && le(b + 10, 2) == 64 && b[12] == 52 && b[13] == 11 &&
-                    b[15] == 52 && le(b + 16, 4) == 1023;
+    } else if (type == 0x01) {
+        return dataspace(b, n, &o->rank, o->dims, &o->count);
+    } else if (type == 0x03) {
+        o->type = dtype_code(b, n);
     } else if (type == 0x08 && n >= 2) {
         if (b[0] != 3) return failf(NULL, "layout message version %d unsupported", b[0]);
         if (b[1] == 1 && n >= 18) {
@@ -766,46 +833,51 @@ static int info_fn(void* ctx, int type, const unsigned char* b, size_t n) {
         } else {
             return failf(NULL, "chunked or virtual datasets unsupported");
         }
+    } else if (type == 0x0C && o->want_attr && n >= 8 && b[0] == 1) {
+        const size_t nl = (size_t)le(b + 2, 2), dl = (size_t)le(b + 4, 2), sl = (size_t)le(b + 6, 2);
+        size_t p = 8;
+        if (p + nl > n || nl == 0 || b[p + nl - 1] != 0) return 0;
+        const int match = strcmp((const char*)b + p, o->want_attr) == 0;
+        p += (nl + 7) & ~(size_t)7;
+        if (!match || p + dl > n) return 0;
+        const int dt = is_ieee_double(b + p, dl) ? NS2D_H5_F64 : -1;
+        p += (dl + 7) & ~(size_t)7;
+        int r;
+        uint64_t dims[8], cnt;
+        if (p + sl > n || dataspace(b + p, sl, &r, dims, &cnt)) return -1;
+        p += (sl + 7) & ~(size_t)7;
+        if (dt != NS2D_H5_F64 || cnt != 1 || p + 8 > n) return failf(NULL, "attribute %s is not one double", o->want_attr);
+        memcpy(&o->attr_value, b + p, 8);
+        o->attr_found = 1;
     }
     return 0;
 }
 
-/* Find `name` in the symbol-table group (btree, heap); *oh receives its
-   header address.  Returns 0 found, 1 absent, -1 on a format error. */
-static int find_in_group(h5_in* in, uint64_t btree, uint64_t heap, const char* name, size_t len, uint64_t* oh,
-                         int leaf_k, int node_k, int depth) {
-    unsigned char hh[32];
+/* Visit the links of the symbol-table group (btree, heap): fn(ctx, name,
+   header address) returns nonzero to stop (1 = found, -1 = error). */
+typedef int (*link_fn)(void* ctx, const char* name, uint64_t oh);
+static int walk_btree(h5_in* in, uint64_t btree, const char* names, uint64_t hsize, link_fn fn, void* ctx, int depth) {
     if (depth > 16) return failf(NULL, "B-tree too deep");
-    if (rd(in, heap, hh, 32) || memcmp(hh, "HEAP", 4) != 0) return failf(NULL, "bad local heap");
-    const uint64_t hsize = le(hh + 8, 8), haddr = le(hh + 24, 8);
-    if (hsize > in->size) return failf(NULL, "bad local heap");
-    const size_t bt_size = 24 + (size_t)(2 * node_k + 1) * 8 + (size_t)(2 * node_k) * 8;
+    const size_t bt_size = 24 + (size_t)(2 * in->node_k + 1) * 8 + (size_t)(2 * in->node_k) * 8;
     unsigned char* node = (unsigned char*)malloc(bt_size);
-    char* names = (char*)malloc((size_t)hsize + 1);
-    int rc = 1;
-    if (!node || !names) {
+    if (!node) return failf(NULL, "out of memory");
+    int rc = 0;
+    if (rd(in, btree, node, bt_size) || memcmp(node, "TREE", 4) != 0 || node[4] != 0) {
         free(node);
-        free(names);
-        return failf(NULL, "out of memory");
+        return failf(NULL, "bad group B-tree");
     }
-    if (rd(in, haddr, names, (size_t)hsize) || rd(in, btree, node, bt_size) || memcmp(node, "TREE", 4) != 0 ||
-        node[4] != 0) {
-        rc = failf(NULL, "bad group B-tree");
-        goto out;
-    }
-    names[hsize] = '\0';
     const int level = node[5], used = (int)le(node + 6, 2);
-    if (used > 2 * node_k) {
-        rc = failf(NULL, "bad group B-tree");
-        goto out;
+    if (used > 2 * in->node_k) {
+        free(node);
+        return failf(NULL, "bad group B-tree");
     }
-    for (int c = 0; c < used && rc == 1; ++c) {
+    const size_t sn_size = 8 + (size_t)(2 * in->leaf_k) * 40;
+    for (int c = 0; c < used && rc == 0; ++c) {
         const uint64_t child = le(node + 24 + 8 + 16 * (size_t)c, 8);
         if (level > 0) {
-            rc = find_in_group(in, child, heap, name, len, oh, leaf_k, node_k, depth + 1);
+            rc = walk_btree(in, child, names, hsize, fn, ctx, depth + 1);
             continue;
         }
-        const size_t sn_size = 8 + (size_t)(2 * leaf_k) * 40;
         unsigned char* sn = (unsigned char*)malloc(sn_size);
         if (!sn || rd(in, child, sn, sn_size) || memcmp(sn, "SNOD", 4) != 0) {
             free(sn);
@@ -813,96 +885,199 @@ static int find_in_group(h5_in* in, uint64_t btree, uint64_t heap, const char* n
             break;
         }
         const int ns = (int)le(sn + 6, 2);
-        for (int e = 0; e < ns && e < 2 * leaf_k; ++e) {
+        for (int e = 0; e < ns && e < 2 * in->leaf_k && rc == 0; ++e) {
             const uint64_t off = le(sn + 8 + 40 * (size_t)e, 8);
-            if (off < hsize && strlen(names + off) == len && memcmp(names + off, name, len) == 0) {
-                *oh = le(sn + 8 + 40 * (size_t)e + 8, 8);
-                rc = 0;
-                break;
-            }
+            if (off < hsize) rc = fn(ctx, names + off, le(sn + 8 + 40 * (size_t)e + 8, 8));
         }
         free(sn);
     }
-out:
     free(node);
+    return rc;
+}
+static int walk_group(h5_in* in, uint64_t btree, uint64_t heap, link_fn fn, void* ctx) {
+    unsigned char hh[32];
+    if (rd(in, heap, hh, 32) || memcmp(hh, "HEAP", 4) != 0) return failf(NULL, "bad local heap");
+    const uint64_t hsize = le(hh + 8, 8), haddr = le(hh + 24, 8);
+    if (hsize > in->size) return failf(NULL, "bad local heap");
+    char* names = (char*)malloc((size_t)hsize + 1);
+    if (!names) return failf(NULL, "out of memory");
+    int rc = rd(in, haddr, names, (size_t)hsize);
+    if (!rc) {
+        names[hsize] = '\0';
+        rc = walk_btree(in, btree, names, hsize, fn, ctx, 0);
+    }
     free(names);
     return rc;
 }
 
-int ns2d_h5_read_double(const char* path, const char* dataset, double* out, uint64_t count) {
-    h5_in in = {0};
-    if (!path || !dataset || !out) return failf(NULL, "invalid arguments");
-    in.fp = fopen(path, "rb");
-    if (!in.fp) return failf(NULL, "cannot open %s: %s", path, strerror(errno));
-    int rc = -1;
-    unsigned char sb[96];
-    fseeko(in.fp, 0, SEEK_END);
-    in.size = (uint64_t)ftello(in.fp);
-    static const unsigned char sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
-    if (rd(&in, 0, sb, 56) || memcmp(sb, sig, 8) != 0) {
-        failf(NULL, "%s is not an HDF5 file (superblock at 0 only)", path);
-        goto out;
+typedef struct find_ctx {
+    const char* name;
+    size_t len;
+    uint64_t oh;
+} find_ctx;
+static int find_fn(void* ctx, const char* name, uint64_t oh) {
+    find_ctx* f = (find_ctx*)ctx;
+    if (strlen(name) == f->len && memcmp(name, f->name, f->len) == 0) {
+        f->oh = oh;
+        return 1;
     }
-    if (sb[8] > 1 || sb[13] != 8 || sb[14] != 8) {
-        failf(NULL, "superblock version %d / offset size %d unsupported", sb[8], sb[13]);
-        goto out;
-    }
-    const int leaf_k = (int)le(sb + 16, 2), node_k = (int)le(sb + 18, 2);
-    const size_t root_at = sb[8] == 0 ? 56 : 60;
-    unsigned char ent[40];
-    if (leaf_k <= 0 || node_k <= 0 || rd(&in, root_at, ent, 40)) {
-        failf(NULL, "bad superblock");
-        goto out;
-    }
-    uint64_t oh = le(ent + 8, 8);
-    const char* s = dataset;
+    return 0;
+}
+
+/* Header address of the object at `path`: 0 found, 1 absent, -1 error. */
+static int locate(h5_in* in, const char* path, uint64_t* oh) {
+    *oh = in->root_oh;
+    const char* s = path;
     for (;;) {
         while (*s == '/') ++s;
-        if (!*s) break;
+        if (!*s) return 0;
         const char* e = strchr(s, '/');
         const size_t len = e ? (size_t)(e - s) : strlen(s);
         obj_info gi;
         memset(&gi, 0, sizeof(gi));
         gi.layout = -1;
-        if (walk_header(&in, oh, info_fn, &gi)) goto out;
-        if (!gi.is_group) {
-            failf(NULL, "%.*s: parent is not a group", (int)len, s);
-            goto out;
-        }
-        int f = find_in_group(&in, gi.btree, gi.heap, s, len, &oh, leaf_k, node_k, 0);
-        if (f) {
-            if (f > 0) failf(NULL, "%s has no object %.*s", path, (int)len, s);
-            goto out;
-        }
+        if (walk_header(in, *oh, info_fn, &gi)) return -1;
+        if (!gi.is_group) return 1;
+        find_ctx fc = {s, len, 0};
+        const int r = walk_group(in, gi.btree, gi.heap, find_fn, &fc);
+        if (r < 0) return -1;
+        if (r == 0) return 1;
+        *oh = fc.oh;
         s += len;
     }
-    obj_info di;
-    memset(&di, 0, sizeof(di));
-    di.layout = -1;
-    if (walk_header(&in, oh, info_fn, &di)) goto out;
-    if (!di.has_type || !di.dbl_ok) {
-        failf(NULL, "%s:%s is not a dataset of IEEE little-endian doubles", path, dataset);
-        goto out;
+}
+
+static int object_info(const char* path, const char* name, obj_info* oi, h5_in* in) {
+    if (!path || !name) return failf(NULL, "invalid arguments");
+    if (open_in(in, path)) {
+        if (in->fp) fclose(in->fp);
+        return -1;
     }
-    if (di.count != count) {
-        failf(NULL, "%s:%s holds %llu values, %llu expected", path, dataset, (unsigned long long)di.count,
-              (unsigned long long)count);
-        goto out;
+    uint64_t oh;
+    const int f = locate(in, name, &oh);
+    if (f) {
+        if (f > 0) failf(NULL, "%s has no object %s", path, name);
+        fclose(in->fp);
+        return -1;
     }
-    if (di.layout == 1) {
-        if (di.data_size != count * 8) {
-            failf(NULL, "%s:%s: storage size differs from the dataspace", path, dataset);
-            goto out;
+    if (walk_header(in, oh, info_fn, oi)) {
+        fclose(in->fp);
+        return -1;
+    }
+    return 0;
+}
+
+int ns2d_h5_dataset_info(const char* path, const char* dataset, int* type, int* rank, uint64_t* dims) {
+    h5_in in;
+    obj_info* oi = (obj_info*)calloc(1, sizeof(obj_info));
+    if (!oi) return failf(NULL, "out of memory");
+    oi->layout = -1;
+    oi->type = -1;
+    int rc = object_info(path, dataset, oi, &in);
+    if (!rc) {
+        fclose(in.fp);
+        if (oi->is_group || oi->layout < 0) {
+            rc = failf(NULL, "%s:%s is not a dataset", path, dataset);
+        } else {
+            if (type) *type = oi->type;
+            if (rank) *rank = oi->rank;
+            if (dims)
+                for (int i = 0; i < oi->rank; ++i) dims[i] = oi->dims[i];
         }
-        if (rd(&in, di.data_addr, out, (size_t)(count * 8))) goto out;
-    } else if (di.layout == 0 && di.compact_size == count * 8) {
-        memcpy(out, di.compact, (size_t)(count * 8));
-    } else {
-        failf(NULL, "%s:%s: no readable storage", path, dataset);
-        goto out;
     }
-    rc = 0;
-out:
-    fclose(in.fp);
+    free(oi);
     return rc;
+}
+
+int ns2d_h5_read(const char* path, const char* dataset, int type, void* out, uint64_t count) {
+    h5_in in;
+    if (!out) return failf(NULL, "invalid arguments");
+    obj_info* oi = (obj_info*)calloc(1, sizeof(obj_info));
+    if (!oi) return failf(NULL, "out of memory");
+    oi->layout = -1;
+    oi->type = -1;
+    int rc = object_info(path, dataset, oi, &in);
+    if (rc) {
+        free(oi);
+        return rc;
+    }
+    const uint64_t bytes = count * type_size(type);
+    rc = -1;
+    if (oi->type != type || oi->type < 0)
+        failf(NULL, "%s:%s does not hold elements of type %d", path, dataset, type);
+    else if (oi->count != count)
+        failf(NULL, "%s:%s holds %llu values, %llu expected", path, dataset, (unsigned long long)oi->count,
+              (unsigned long long)count);
+    else if (oi->layout == 1 && oi->data_size == bytes)
+        rc = rd(&in, oi->data_addr, out, (size_t)bytes);
+    else if (oi->layout == 0 && oi->compact_size == bytes) {
+        memcpy(out, oi->compact, (size_t)bytes);
+        rc = 0;
+    } else
+        failf(NULL, "%s:%s: no readable storage", path, dataset);
+    fclose(in.fp);
+    free(oi);
+    return rc;
+}
+
+int ns2d_h5_read_double(const char* path, const char* dataset, double* out, uint64_t count) {
+    return ns2d_h5_read(path, dataset, NS2D_H5_F64, out, count);
+}
+
+int ns2d_h5_read_attr_double(const char* path, const char* object, const char* name, double* value) {
+    h5_in in;
+    if (!name || !value) return failf(NULL, "invalid arguments");
+    obj_info* oi = (obj_info*)calloc(1, sizeof(obj_info));
+    if (!oi) return failf(NULL, "out of memory");
+    oi->layout = -1;
+    oi->want_attr = name;
+    int rc = object_info(path, object, oi, &in);
+    if (!rc) {
+        fclose(in.fp);
+        if (oi->attr_found)
+            *value = oi->attr_value;
+        else
+            rc = failf(NULL, "%s:%s has no attribute %s", path, object, name);
+    }
+    free(oi);
+    return rc;
+}
+
+typedef struct list_ctx {
+    char* buf;
+    size_t cap, used;
+    int n;
+} list_ctx;
+static int list_fn(void* ctx, const char* name, uint64_t oh) {
+    (void)oh;
+    list_ctx* l = (list_ctx*)ctx;
+    const size_t len = strlen(name);
+    if (l->used + len + 1 > l->cap) return failf(NULL, "name buffer too small");
+    memcpy(l->buf + l->used, name, len);
+    l->buf[l->used + len] = '\n';
+    l->used += len + 1;
+    l->n++;
+    return 0;
+}
+
+int ns2d_h5_list(const char* path, const char* group, char* buf, size_t cap) {
+    h5_in in;
+    if (!buf || cap == 0) return failf(NULL, "invalid arguments");
+    obj_info* oi = (obj_info*)calloc(1, sizeof(obj_info));
+    if (!oi) return failf(NULL, "out of memory");
+    oi->layout = -1;
+    int rc = object_info(path, group, oi, &in);
+    if (rc) {
+        free(oi);
+        return rc;
+    }
+    list_ctx l = {buf, cap - 1, 0, 0};
+    if (!oi->is_group)
+        rc = failf(NULL, "%s:%s is not a group", path, group);
+    else if (walk_group(&in, oi->btree, oi->heap, list_fn, &l) != 0)
+        rc = -1;
+    buf[l.used] = '\0';
+    fclose(in.fp);
+    free(oi);
+    return rc ? -1 : l.n;
 }

@@ -45,7 +45,7 @@ class Params(C.Structure):
         ("adapt_step_flag", C.c_int32), ("cfl_cond_flag", C.c_int32),
         ("cfl_const", C.c_double), ("dt", C.c_double),
         ("precision", C.c_int32), ("flux_diagnostics", C.c_int32),
-        ("device", C.c_int32), ("reserved", C.c_int32),
+        ("device", C.c_int32), ("dealias_edge", C.c_int32),
     ]
 
     def copy(self):
@@ -68,6 +68,22 @@ class Measures(C.Structure):
 
 MEASURE_NAMES = [n for n, _ in Measures._fields_]
 SPECTRA_NAMES = ["enrg", "enst", "d_enst_dt", "enst_flux", "enst_diss", "d_enrg_dt", "enrg_flux", "enrg_diss"]
+
+
+# Parameter files written before the last int32 of ns2d_params was named
+# dealias_edge call it "reserved" (its value was always 0).
+_RENAMED = {"reserved": "dealias_edge"}
+
+
+def params_from_arrays(names, values):
+    """ns2d_params from parallel arrays of field names and values (the golden
+    fixtures' param_names / params)."""
+    types = dict(Params._fields_)
+    kw = {}
+    for n, v in zip(names, values):
+        n = _RENAMED.get(str(n), str(n))
+        kw[n] = float(v) if types[n].__name__ == "c_double" else int(v)
+    return default_params(**kw)
 
 
 def default_params(**kw):
@@ -95,7 +111,7 @@ def default_params(**kw):
     p.precision = FP64
     p.flux_diagnostics = 1
     p.device = 0
-    p.reserved = 0
+    p.dealias_edge = 0
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(f"ns2d_params has no field {k!r}")

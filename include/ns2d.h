@@ -98,7 +98,11 @@ typedef struct ns2d_params {
     int32_t flux_diagnostics; /* 1 = the stock dataset flags (__ENST_FLUX...): the
                                  measurables call evaluates the RHS of the state     */
     int32_t device;           /* CUDA device ordinal                                  */
-    int32_t reserved;
+    int32_t dealias_edge;     /* 2/3 rule edge: 0 = zero |k| >= (int)(N/3), the
+                                 solver's ApplyDealiasing (solver.c:1049-1068);
+                                 1 = zero |k| > (int)(N/3), the post-processing
+                                 program's (PostProcessing/src/full_field.c:128);
+                                 single handles only                          */
 } ns2d_params;
 
 /* Scalars of ComputeSystemMeasurables (Solver/src/sys_msr.c:32-373), in order. */

@@ -20,6 +20,7 @@
  */
 #ifndef NS2D_H5_H
 #define NS2D_H5_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -60,13 +61,24 @@ int ns2d_h5_flush(ns2d_h5_file* f);
 /* Flush and close.  Returns -1 (after releasing f) if the flush failed. */
 int ns2d_h5_close(ns2d_h5_file* f);
 
-/* Read the dataset `dataset` ("/psi") of `count` doubles from an existing
-   HDF5 file into out (C order), for initial conditions read from file
-   (Solver/src/solver.c:1775-1853, H5LTread_dataset_double).  Handles files in
-   libhdf5's default layout (superblock 0/1, symbol-table groups, v1 object
-   headers, contiguous or compact storage of IEEE little-endian doubles).
-   0 on success; -1 with ns2d_h5_error(NULL) set otherwise. */
+/* Reading existing files in libhdf5's default layout (superblock 0/1,
+   symbol-table groups, v1 object headers, contiguous or compact storage) --
+   input files (MAX_PALIN, Solver/src/solver.c:1775-1853) and saved runs for
+   post-processing (PostProcessing/src/hdf5_funcs.c:33-170).  All return 0 (or
+   a count) on success and -1 with ns2d_h5_error(NULL) set otherwise; each call
+   opens and closes the file. */
+
+/* Element type (NS2D_H5_*, -1 for others), rank and dimensions (<= 8) of a dataset. */
+int ns2d_h5_dataset_info(const char* path, const char* dataset, int* type, int* rank, uint64_t* dims);
+/* `count` elements of type NS2D_H5_* (H5LTread_dataset) into out, C order. */
+int ns2d_h5_read(const char* path, const char* dataset, int type, void* out, uint64_t count);
+/* ns2d_h5_read of doubles (H5LTread_dataset_double). */
 int ns2d_h5_read_double(const char* path, const char* dataset, double* out, uint64_t count);
+/* A one-double attribute of the object at `object` (H5LTget_attribute_double). */
+int ns2d_h5_read_attr_double(const char* path, const char* object, const char* name, double* value);
+/* The link names of group `group`, each followed by '\n', into buf (cap
+   bytes, NUL-terminated); returns how many. */
+int ns2d_h5_list(const char* path, const char* group, char* buf, size_t cap);
 
 /* Message of the last failure on f (or, for NULL, of the last failed create,
    close or read). */

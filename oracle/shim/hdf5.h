@@ -8,6 +8,7 @@
  */
 #ifndef NS2D_SHIM_HDF5_H
 #define NS2D_SHIM_HDF5_H
+#include <stdbool.h> /* libhdf5's public headers bring in bool */
 #include <stddef.h>
 #include <stdint.h>
 #include "mpi.h"

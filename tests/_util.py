@@ -15,12 +15,7 @@ from ns2d import abi  # noqa: E402
 
 def load_case(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
-    names = [str(s) for s in z["param_names"]]
-    kw = {}
-    for n, v in zip(names, z["params"]):
-        t = dict(abi.Params._fields_)[n]
-        kw[n] = float(v) if t.__name__ == "c_double" else int(v)
-    p = abi.default_params(**kw)
+    p = abi.params_from_arrays(z["param_names"], z["params"])
     outs = [z[f"out{i}"] for i in range(int(z["n_out"]))]
     return p, z["w0"], outs
 

@@ -121,10 +121,7 @@ def test_checkpoint_interval_does_not_change_gradient():
 
 def test_restatement_matches_reference_tangent_linear_fixture():
     z = np.load(os.path.join(GOLDEN, "adjoint32_tl.npz"))
-    names = [str(s) for s in z["param_names"]]
-    kw = {n: (float(v) if dict(abi.Params._fields_)[n].__name__ == "c_double" else int(v))
-          for n, v in zip(names, z["params"])}
-    p = abi.default_params(**kw)
+    p = abi.params_from_arrays(z["param_names"], z["params"])
     m = ar.Model(p.nx, ar.bracket_for(p))
     nsteps = int(z["nsteps"])
     Z, gZ = m.gradient(z["w0"], nsteps, p.dt, "enstrophy", checkpoint_every=10)

@@ -67,10 +67,7 @@ def test_hou_li_kolmogorov_palinstrophy():
 
 def test_reference_tangent_linear_fixture():
     z = np.load(os.path.join(GOLDEN, "adjoint32_tl.npz"))
-    names = [str(x) for x in z["param_names"]]
-    kw = {k: (float(v) if dict(abi.Params._fields_)[k].__name__ == "c_double" else int(v))
-          for k, v in zip(names, z["params"])}
-    p = abi.default_params(**kw)
+    p = abi.params_from_arrays(z["param_names"], z["params"])
     nsteps = int(z["nsteps"])
     for kind, key, dkey in ((abi.OBJ_ENSTROPHY, "Z", "dZ"), (abi.OBJ_PALINSTROPHY, "P", "dP")):
         s = Solver(p)

@@ -176,3 +176,46 @@ def test_reader_rejects_corruption(h5, tmp_path):
     open(fn, "wb").write(bytes(raw))
     with pytest.raises(h5read.H5FormatError):
         h5read.read(fn)
+
+
+def test_reader_types_attributes_and_listing(h5, tmp_path):
+    """The reading side a post-processor needs: dataset shapes and types,
+    complex and int datasets, group attributes, and a group's link names
+    (past a multi-level index)."""
+    L = h5
+    L.ns2d_h5_dataset_info.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_uint64)]
+    L.ns2d_h5_read.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_void_p, C.c_uint64]
+    L.ns2d_h5_read_attr_double.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_double)]
+    L.ns2d_h5_list.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t]
+    fn = str(tmp_path / "run.h5")
+    f = L.ns2d_h5_create(fn.encode())
+    rng = np.random.default_rng(9)
+    wh = rng.standard_normal((8, 5)) + 1j * rng.standard_normal((8, 5))
+    for it in range(300):
+        g = f"/Iter_{it:05d}".encode()
+        assert L.ns2d_h5_group(f, g) == 0
+        assert L.ns2d_h5_attr_double(f, g, b"TimeValue", 0.5 * it) == 0
+    assert _ds(L, f, "/Iter_00299/w_hat", wh, C128) == 0
+    assert _ds(L, f, "/kx", np.arange(-3, 5, dtype=np.int32), I32) == 0
+    assert L.ns2d_h5_close(f) == 0
+    t, r, dims = C.c_int(), C.c_int(), (C.c_uint64 * 8)()
+    assert L.ns2d_h5_dataset_info(fn.encode(), b"/Iter_00299/w_hat", C.byref(t), C.byref(r), dims) == 0
+    assert (t.value, r.value, dims[0], dims[1]) == (C128, 2, 8, 5)
+    out = np.zeros((8, 5), dtype=np.complex128)
+    assert L.ns2d_h5_read(fn.encode(), b"/Iter_00299/w_hat", C128, out.ctypes.data, out.size) == 0
+    assert np.array_equal(out, wh)
+    assert L.ns2d_h5_read(fn.encode(), b"/Iter_00299/w_hat", F64, out.ctypes.data, out.size) == -1
+    ints = np.zeros(8, dtype=np.int32)
+    assert L.ns2d_h5_read(fn.encode(), b"/kx", I32, ints.ctypes.data, 8) == 0
+    assert np.array_equal(ints, np.arange(-3, 5))
+    v = C.c_double()
+    assert L.ns2d_h5_read_attr_double(fn.encode(), b"/Iter_00123", b"TimeValue", C.byref(v)) == 0
+    assert v.value == 61.5
+    assert L.ns2d_h5_read_attr_double(fn.encode(), b"/Iter_00123", b"Nope", C.byref(v)) == -1
+    buf = C.create_string_buffer(1 << 16)
+    assert L.ns2d_h5_list(fn.encode(), b"/", buf, len(buf)) == 301
+    names = buf.value.decode().split("\n")[:-1]
+    assert names == sorted([f"Iter_{i:05d}" for i in range(300)] + ["kx"])
+    assert L.ns2d_h5_list(fn.encode(), b"/", buf, 16) == -1  # too small
+    assert L.ns2d_h5_list(fn.encode(), b"/kx", buf, len(buf)) == -1  # not a group
