@@ -655,6 +655,17 @@ ns2d_status rk4_step_loop(ns2d_handle* h, double dt) {
     return NS2D_OK;
 }
 
+// One step for the per-call entry points (ns2d_rk4_step, ns2d_rk4_step_host):
+// eager when dt differs from the previous call's (adaptive stepping would
+// recapture every step), the graph-replayed step of the time loops when the
+// same dt comes again.  Both run the same kernels on the same arguments.
+ns2d_status single_step(ns2d_handle* h, double dt) {
+    const bool again = (h->last_call_dt == dt);
+    h->last_call_dt = dt;
+    if (again) return rk4_step_loop(h, dt);
+    return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+}
+
 ns2d_status host_to_state(ns2d_handle* h, const double* host, void* dst) {
     CK(h, cudaMemcpyAsync(h->dio, host, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyHostToDevice, h->stream));
     return DISPATCH(h, pack_in, h, h->dio, dst);
@@ -1007,7 +1018,7 @@ ns2d_status ns2d_nonlinear_rhs(ns2d_handle* h, const double* in, double* out) {
 ns2d_status ns2d_rk4_step(ns2d_handle* h, double dt) {
     if (!h) return NS2D_ERR_INVALID;
     cudaSetDevice(h->p.device);
-    ns2d_status s = DISPATCH(h, rk4_step_impl, h, dt, nullptr);
+    ns2d_status s = single_step(h, dt);
     if (s) return s;
     return check_status(h);
 }
@@ -1229,7 +1240,7 @@ ns2d_status ns2d_rk4_step_host(ns2d_handle* h, double* w_hat, double dt) {
     cudaSetDevice(h->p.device);
     ns2d_status s = host_to_state(h, w_hat, h->state);
     if (s) return s;
-    if ((s = DISPATCH(h, rk4_step_impl, h, dt, nullptr))) return s;
+    if ((s = single_step(h, dt))) return s;
     if ((s = state_to_host(h, h->state, w_hat))) return s;
     return check_status(h);
 }

@@ -77,6 +77,7 @@ struct ns2d_handle {
     int graph_kernels = 9;  // kernels in one captured step
     double graph_dt = 0.0;
     int graph_branch = -1;
+    double last_call_dt = -1.0;  // dt of the previous ns2d_rk4_step / _host call
     // the same with an event pair around every launch (kernel timing mode)
     cudaGraphExec_t timed_graph = nullptr;
     double timed_dt = 0.0;
