@@ -186,6 +186,31 @@ def test_blowup_exits_with_status_1_and_valid_files(tmp_path):
         _close(got[k], want[k], k)
 
 
+@pytest.mark.parametrize("variant,extra", [("rk4", "--integrator=RK4"), ("houli", "--dealias=HOU_LI")])
+@pytest.mark.parametrize("case", ["decay_fixed", "decay_adaptive", "tg_drag", "stoc"])
+def test_compile_time_variants_match_reference_program(variant, extra, case, tmp_path):
+    """The reference program built with -D__RK4 (explicit RK4 with its
+    linear-term quirk) or with Hou-Li dealiasing (its header switched to
+    __DEALIAS_HOU_LI) against bin/ns2d with the matching run-time option."""
+    exe = REF + "_" + variant
+    if not os.path.exists(exe):
+        pytest.skip("variant of the reference program not built")
+    args = f"{BASE} {CASES[case]} -o out/"
+    (tmp_path / "ref").mkdir()
+    (tmp_path / "gpu").mkdir()
+    _run(exe, args, tmp_path / "ref")
+    _run(NS2D, args, tmp_path / "gpu", ["--quiet", extra])
+    rdirs = sorted(os.listdir(tmp_path / "ref" / "out"))
+    assert rdirs == sorted(os.listdir(tmp_path / "gpu" / "out")) and len(rdirs) == 1
+    bad = []
+    for fname in FILES:
+        want, _, _ = h5log.read(str(tmp_path / "ref" / "out" / rdirs[0] / fname))
+        got, _ = h5read.flatten(h5read.read(str(tmp_path / "gpu" / "out" / rdirs[0] / fname)))
+        assert set(got) == set(want)
+        bad += _compare_file(got, want, fname)
+    assert not bad, bad[:20]
+
+
 @pytest.mark.parametrize("extra", [["--integrator=RK4"], ["--integrator=AB4"], ["--integrator=DP5"],
                                    ["--precision=FP32"], ["--dealias=HOU_LI"]])
 def test_variants_run(extra, tmp_path):
