@@ -20,6 +20,7 @@
  * options select what the reference fixes when it is compiled:
  * --integrator=RK4CN|RK4|AB4|DP5, --dealias=23|HOU_LI, --precision=FP64|FP32,
  * --device=N, --no-quirks (corrected forms of the reference's quirks),
+ * --phase-only (the -D__PHASE_ONLY model, RK4CN / RK4 only),
  * --dry-run (print the parameters as JSON and exit), --quiet.
  */
 #include <getopt.h>
@@ -60,7 +61,7 @@ static void usage_and_exit(void) {
             "Use -p to specify how often to print to file\n"
             "Use -z to specify an input file to read parameters from\n"
             "Long options: --integrator=RK4CN|RK4|AB4|DP5 --dealias=23|HOU_LI --precision=FP64|FP32\n"
-            "              --device=N --no-quirks --dry-run --quiet\n"
+            "              --device=N --no-quirks --phase-only --dry-run --quiet\n"
             "\nExample usage:\n\tns2d -o ../Data/Tmp/ -n 64 -n 64 -s 0.0 -e 1.0 -h 0.0001 -v 1.0 -i TG_VORT -t TEMP_RUN\n"
             "-->> Now Exiting!\n\n");
     exit(1);
@@ -129,7 +130,8 @@ static void defaults(ns2d_run* r) {
     r->quirks = NS2D_QUIRKS_REFERENCE;
 }
 
-enum { OPT_INTEGRATOR = 1000, OPT_DEALIAS, OPT_PRECISION, OPT_DEVICE, OPT_NO_QUIRKS, OPT_DRY_RUN, OPT_QUIET };
+enum { OPT_INTEGRATOR = 1000, OPT_DEALIAS, OPT_PRECISION, OPT_DEVICE, OPT_NO_QUIRKS, OPT_DRY_RUN, OPT_QUIET,
+       OPT_PHASE_ONLY };
 
 void ns2d_cli_parse(int argc, char** argv, ns2d_run* r) {
     static const struct option longs[] = {{"integrator", required_argument, 0, OPT_INTEGRATOR},
@@ -139,6 +141,7 @@ void ns2d_cli_parse(int argc, char** argv, ns2d_run* r) {
                                           {"no-quirks", no_argument, 0, OPT_NO_QUIRKS},
                                           {"dry-run", no_argument, 0, OPT_DRY_RUN},
                                           {"quiet", no_argument, 0, OPT_QUIET},
+                                          {"phase-only", no_argument, 0, OPT_PHASE_ONLY},
                                           {0, 0, 0, 0}};
     defaults(r);
     int seen_o = 0, seen_n = 0, seen_h = 0, seen_c = 0, seen_v = 0, seen_d = 0, seen_f = 0, seen_T = 0;
@@ -275,8 +278,14 @@ void ns2d_cli_parse(int argc, char** argv, ns2d_run* r) {
             case OPT_QUIET:
                 r->quiet = 1;
                 break;
+            case OPT_PHASE_ONLY:
+                r->phase_only = 1;
+                break;
             default:
                 usage_and_exit();
         }
     }
+    /* the phase-only reset exists in RK4Step only (solver.c:822-857) */
+    if (r->phase_only && r->integrator != NS2D_RK4CN && r->integrator != NS2D_RK4)
+        die_str("--phase-only needs --integrator=RK4CN or RK4%s", "");
 }

@@ -64,12 +64,12 @@ static void print_json(const ns2d_run* r) {
            "\"trans_iters\": %d, \"trans_frac\": %.17g, \"nu\": %.17g, \"hyper_flag\": %d, \"hyper_pow\": %.17g, "
            "\"ekmn_alpha\": %.17g, \"ekmn_flag\": %d, \"ekmn_pow\": %.17g, \"save_every\": %d, \"output_dir\": \"%s\", "
            "\"output_tag\": \"%s\", \"input_file\": \"%s\", \"file_only\": %d, \"integrator\": \"%s\", "
-           "\"dealias\": \"%s\", \"precision\": \"%s\", \"quirks\": %d}\n",
+           "\"dealias\": \"%s\", \"precision\": \"%s\", \"quirks\": %d, \"phase_only\": %d}\n",
            r->N[0], r->N[1], r->t0, r->T, r->dt, r->adapt_step, r->cfl_cond, r->cfl_const, r->u0, r->forcing,
            r->force_k, r->force_scale, r->trans_iters, r->trans_frac, r->nu, r->hyper_flag, r->hyper_pow,
            r->ekmn_alpha, r->ekmn_flag, r->ekmn_pow, r->save_every, r->output_dir, r->output_tag, r->input_file,
            r->file_only, integrator_name(r->integrator), r->dealias == NS2D_DEALIAS_HOU_LI ? "HOU_LI" : "23",
-           r->precision == NS2D_FP32 ? "FP32" : "FP64", r->quirks);
+           r->precision == NS2D_FP32 ? "FP32" : "FP64", r->quirks, r->phase_only);
 }
 
 /* ---- run state ------------------------------------------------------------------ */
@@ -155,8 +155,43 @@ static void group(ns2d_h5_file* f, const char* name, double t, double dt) {
     h5check(ns2d_h5_attr_double(f, name, "TimeStep", dt), f, name);
 }
 
-/* The datasets of one save (WriteDataToFile, hdf5_funcs.c:650-1050). */
-static void write_save(state* s, double t, double dt, long idx) {
+/* Fourier amplitudes and phases of the phase-only model, "a_k" = |w_hat| and
+   "phi_k" = arg w_hat on [nx][nyf] (WriteDataToFile, hdf5_funcs.c:899-925).
+   The initial save of the reference (hdf5_funcs.c:264-290) indexes both
+   arrays by the row alone, so entry i holds mode (i, nyf-1) and the rest stay
+   0; that form is kept with the reference's quirks on. */
+static void write_amplitudes_phases(state* s, const char* gname, int initial) {
+    const size_t n = (size_t)(s->nx * s->nyf);
+    double* a = (double*)calloc(2 * n, sizeof(double));
+    if (!a) {
+        fprintf(stderr, "out of memory\n");
+        exit(1);
+    }
+    double* phi = a + n;
+    if (initial && s->r->quirks) {
+        for (long i = 0; i < s->nx; ++i) {
+            const double complex w = s->w_hat[(size_t)i * s->nyf + s->nyf - 1];
+            a[i] = cabs(w);
+            phi[i] = carg(w);
+        }
+    } else {
+        for (size_t q = 0; q < n; ++q) {
+            a[q] = cabs(s->w_hat[q]);
+            phi[q] = carg(s->w_hat[q]);
+        }
+    }
+    const uint64_t df[2] = {(uint64_t)s->nx, (uint64_t)s->nyf};
+    char path[128];
+    snprintf(path, sizeof(path), "%s/a_k", gname);
+    h5check(ns2d_h5_dataset(s->fmain, path, NS2D_H5_F64, 2, df, a), s->fmain, path);
+    snprintf(path, sizeof(path), "%s/phi_k", gname);
+    h5check(ns2d_h5_dataset(s->fmain, path, NS2D_H5_F64, 2, df, phi), s->fmain, path);
+    free(a);
+}
+
+/* The datasets of one save (WriteDataToFile, hdf5_funcs.c:650-1050; `initial`:
+   the initial condition's, CreateOutputFilesWriteICs, hdf5_funcs.c:200-300). */
+static void write_save(state* s, double t, double dt, long idx, int initial) {
     char gname[64], path[128];
     snprintf(gname, sizeof(gname), "/Iter_%05d", (int)idx);
     group(s->fmain, gname, t, dt);
@@ -168,6 +203,7 @@ static void write_save(state* s, double t, double dt, long idx) {
     h5check(ns2d_h5_dataset(s->fmain, path, NS2D_H5_F64, 2, dr, s->w_real), s->fmain, path);
     snprintf(path, sizeof(path), "%s/w_hat", gname);
     h5check(ns2d_h5_dataset(s->fmain, path, NS2D_H5_C128, 2, df, s->w_hat), s->fmain, path);
+    if (s->r->phase_only) write_amplitudes_phases(s, gname, initial);
     const uint64_t ds[1] = {(uint64_t)s->n_spect};
     for (int k = 0; k < 8; ++k) {
         const int q = k_spectra_order[k];
@@ -194,9 +230,9 @@ static void output_paths(state* s) {
     if (r->file_only) {
         if (!r->quiet) printf("\n[NOTE] --- File only output option selected...\n");
         snprintf(data, sizeof(data),
-                 "_SIM[NAV-%s-FULL]_N[%ld,%ld]_T[%1.1lf,%g,%1.3lf]_NU[%g,%d,%1.1lf]_DRAG[%g,%d,%1.1lf]_CFL[%1.2lf]_"
+                 "_SIM[NAV-%s-%s]_N[%ld,%ld]_T[%1.1lf,%g,%1.3lf]_NU[%g,%d,%1.1lf]_DRAG[%g,%d,%1.1lf]_CFL[%1.2lf]_"
                  "FORC[%s,%d,%g]_u0[%s].h5",
-                 integrator_name(r->integrator), r->N[0], r->N[1], r->t0, r->dt, r->T, r->nu, r->hyper_flag,
+                 integrator_name(r->integrator), r->phase_only ? "PO" : "FULL", r->N[0], r->N[1], r->t0, r->dt, r->T, r->nu, r->hyper_flag,
                  r->hyper_pow, r->ekmn_alpha, r->ekmn_flag, r->ekmn_pow, r->cfl_const, r->forcing, r->force_k,
                  r->force_scale, r->u0);
         snprintf(s->main_file, sizeof(s->main_file), "%sMain_HDF_Data%s", r->output_dir, data);
@@ -205,9 +241,9 @@ static void output_paths(state* s) {
         snprintf(s->msr_file, sizeof(s->msr_file), "%sSystemMeasures_HDF_Data%s", r->output_dir, data);
     } else {
         snprintf(data, sizeof(data),
-                 "SIM_DATA_NAVIER_%s_FULL_N[%ld,%ld]_T[%1.1lf,%g,%1.3lf]_NU[%g,%d,%1.1lf]_DRAG[%g,%d,%1.1lf]_"
+                 "SIM_DATA_NAVIER_%s_%s_N[%ld,%ld]_T[%1.1lf,%g,%1.3lf]_NU[%g,%d,%1.1lf]_DRAG[%g,%d,%1.1lf]_"
                  "CFL[%1.2lf]_FORC[%s,%d,%g]_u0[%s]_TAG[%s]/",
-                 integrator_name(r->integrator), r->N[0], r->N[1], r->t0, r->dt, r->T, r->nu, r->hyper_flag,
+                 integrator_name(r->integrator), r->phase_only ? "PHAEONLY" : "FULL", r->N[0], r->N[1], r->t0, r->dt, r->T, r->nu, r->hyper_flag,
                  r->hyper_pow, r->ekmn_alpha, r->ekmn_flag, r->ekmn_pow, r->cfl_const, r->forcing, r->force_k,
                  r->force_scale, r->u0, r->output_tag);
         if (strlen(r->output_dir) + strlen(data) >= sizeof(r->output_dir)) {
@@ -311,7 +347,8 @@ static void simulation_details(state* s, int argc, char** argv, double sim_time,
     fprintf(f, "Executing Command:\n\n\t");
     for (int i = 0; i < argc; ++i) fprintf(f, "%s ", argv[i]);
     fprintf(f, "\n\n");
-    fprintf(f, "Systen Type: NAVIER\nSolver Type: %s\nModel Type: FULL\n", integrator_name(r->integrator));
+    fprintf(f, "Systen Type: NAVIER\nSolver Type: %s\nModel Type: %s\n", integrator_name(r->integrator),
+            r->phase_only ? "PHAEONLY" : "FULL");
     fprintf(f, "Viscosity: %1.6lf\n", r->nu);
     fprintf(f, "Re: %5.1lf\n", 1.0 / r->nu);
     fprintf(f, "Ekman Drag: %s\n", r->ekmn_flag ? "YES" : "NO");
@@ -409,6 +446,7 @@ int main(int argc, char** argv) {
     p.precision = run.precision;
     p.flux_diagnostics = 1;
     p.device = run.device;
+    p.model = run.phase_only ? NS2D_MODEL_PHASE_ONLY : NS2D_MODEL_FULL;
     check(ns2d_create(&p, &g_h), "ns2d_create");
 
     /* InitialConditions + InitializeForcing (solver.c:1107, force.c:28) */
@@ -466,7 +504,7 @@ int main(int argc, char** argv) {
     if (!s.fmain) h5check(-1, NULL, s.main_file);
     s.fspect = ns2d_h5_create(s.spect_file);
     if (!s.fspect) h5check(-1, NULL, s.spect_file);
-    if (!run.trans_iters) write_save(&s, 0.0, dt, 0);
+    if (!run.trans_iters) write_save(&s, 0.0, dt, 0, 1);
 
     /* SpectralSolve's loop (solver.c:127-236) */
     const int listed = fm.kind != 0;
@@ -518,7 +556,7 @@ int main(int argc, char** argv) {
             advance(&s, &pending, dt, iters);
             measurables(&s, t, save_idx);
             if (iters > s.trans_steps) {
-                write_save(&s, t, dt, save_idx);
+                write_save(&s, t, dt, save_idx, 0);
                 save_idx++;
             }
         }

@@ -46,6 +46,7 @@ typedef struct ns2d_run {
     int precision;   /* ns2d_precision */
     int device;
     int quirks;      /* NS2D_QUIRK_* bits, default all */
+    int phase_only;  /* -D__PHASE_ONLY model (ns2d_model)    */
     int dry_run;     /* print the parsed parameters and exit */
     int quiet;
 } ns2d_run;

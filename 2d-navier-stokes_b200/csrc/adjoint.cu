@@ -207,6 +207,8 @@ ns2d_status ensure_buffers(ns2d_handle* h, int nsteps, int every) {
 ns2d_status validate(ns2d_handle* h) {
     if (h->p.system != NS2D_NAVIER || h->p.integrator != NS2D_RK4CN)
         return fail(h, NS2D_ERR_UNSUPPORTED, "the adjoint covers the Navier-Stokes RK4CN step");
+    if (h->p.model != NS2D_MODEL_FULL)
+        return fail(h, NS2D_ERR_UNSUPPORTED, "the adjoint linearises the full model's step, not the phase-only one");
     if (h->p.quirks & NS2D_QUIRK_CONJ_STATE)
         return fail(h, NS2D_ERR_UNSUPPORTED,
                     "the adjoint differentiates the corrected ForceConjugacy: clear NS2D_QUIRK_CONJ_STATE");

@@ -92,6 +92,7 @@ void fill_common(ns2d_handle* h, ColArgs<Real>& a, int branch) {
     a.force_field = h->ffield_on ? (const C*)h->ffield : nullptr;
     a.ntiles = (h->nyf + col_tc(h->nx) - 1) / col_tc(h->nx);
     a.lin = make_lin(h, branch);
+    a.phase_only = h->p.model == NS2D_MODEL_PHASE_ONLY ? 1 : 0;
 }
 
 template <typename Real>
@@ -886,8 +887,11 @@ ns2d_status ns2d_create(const ns2d_params* p, ns2d_handle** out) {
     if (!is_pow2(p->nx) || p->nx < 16 || p->nx > 2048) return NS2D_ERR_UNSUPPORTED;
     if (p->integrator < 0 || p->integrator > 3 || p->dealias < 0 || p->dealias > 1 || p->forcing < 0 ||
         p->forcing > 2 || (p->precision != NS2D_FP64 && p->precision != NS2D_FP32) || p->dealias_edge < 0 ||
-        p->dealias_edge > 1)
+        p->dealias_edge > 1 || p->model < 0 || p->model > 1)
         return NS2D_ERR_INVALID;
+    // phase-only: RK4Step's reset only (solver.c:822-857)
+    if (p->model == NS2D_MODEL_PHASE_ONLY && p->integrator != NS2D_RK4CN && p->integrator != NS2D_RK4)
+        return NS2D_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NS2D_ERR_NO_DEVICE;
     if (p->device < 0 || p->device >= ndev) return NS2D_ERR_INVALID;
@@ -1026,6 +1030,7 @@ ns2d_status ns2d_rk4_step(ns2d_handle* h, double dt) {
 ns2d_status ns2d_ab4_step(ns2d_handle* h, double dt, int32_t iters) {
     if (!h || iters < 1) return NS2D_ERR_INVALID;
     cudaSetDevice(h->p.device);
+    if (h->p.model != NS2D_MODEL_FULL) return fail(h, NS2D_ERR_UNSUPPORTED, "AB4Step has no phase-only form");
     ns2d_status s;
     if (iters <= 3) {
         // start-up: RK4CN step storing RK1 in AB_tmp_nonlin[iters-1] (solver.c:276-284)
@@ -1310,6 +1315,7 @@ ns2d_status ns2d_set_forcing_modes(ns2d_handle* h, int32_t n, const int32_t* idx
 ns2d_status ns2d_dp5_step(ns2d_handle* h, double dt, double* err) {
     if (!h || !err || !(dt > 0.0)) return NS2D_ERR_INVALID;
     cudaSetDevice(h->p.device);
+    if (h->p.model != NS2D_MODEL_FULL) return fail(h, NS2D_ERR_UNSUPPORTED, "the DP5 step has no phase-only form");
     ns2d_status s = DISPATCH(h, dp5_step_impl, h, dt, err);
     if (s) return s;
     return check_status(h);

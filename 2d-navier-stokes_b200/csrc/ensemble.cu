@@ -439,6 +439,7 @@ ns2d_status ns2d_ensemble_create(const ns2d_params* base, int32_t n_members, con
     if (base->integrator != NS2D_RK4CN && base->integrator != NS2D_RK4) return NS2D_ERR_UNSUPPORTED;
     if (base->forcing == NS2D_FORCING_ZERO) return NS2D_ERR_UNSUPPORTED;  // mode killing: single handles only
     if (base->dealias_edge != 0) return NS2D_ERR_UNSUPPORTED;            // the solver's 2/3 edge only
+    if (base->model != NS2D_MODEL_FULL) return NS2D_ERR_UNSUPPORTED;     // phase-only: single handles
     if (base->precision != NS2D_FP64 && base->precision != NS2D_FP32) return NS2D_ERR_INVALID;
     for (int m = 0; m < n_members; ++m)
         if (!ens_size_ok(sizes[m])) return NS2D_ERR_UNSUPPORTED;

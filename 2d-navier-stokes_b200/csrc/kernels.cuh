@@ -103,6 +103,7 @@ struct ColArgs {
     const C* force_field;  // forcing added to every mode of the RHS ([nx][ldc]), may be null
     double inv_nxny;     // 1/(Nx Ny)
     int final_tail;      // COL_FINAL: 1 = SystemCheck bound over ntiles tiles, 0 = non-finite check only
+    int phase_only;      // COL_FINAL: rescale each updated mode k != 0 to the amplitude it had before
     int ntiles;          // number of column tiles of this field
     int* status;         // [0] status bits (kernels return early when set), [1] completed steps
 };
@@ -386,6 +387,15 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                         // Crank-Nicolson factors (solver.c:853), from the table
                         const double2 f = a.cn[(size_t)i * ldc + kyc];
                         wn = cadd(cscale(w, (Real)f.x), cscale(tot, (Real)f.y));
+                    }
+                    if (a.phase_only && (kx != 0 || ky != 0)) {
+                        // amplitude reset of the phase-only model (solver.c:822-824, 855-857):
+                        // w_new *= |w_old| / |w_new|; a mode updated to exactly 0 stays 0
+                        const double an = hypot((double)wn.x, (double)wn.y);
+                        if (an > 0.0) {
+                            const double r = hypot((double)w.x, (double)w.y) / an;
+                            wn = cmake<C>((Real)((double)wn.x * r), (Real)((double)wn.y * r));
+                        }
                     }
                     if (valid) {
                         a.state[(size_t)i * ldc + ky] = wn;

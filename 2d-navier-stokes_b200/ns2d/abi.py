@@ -5,7 +5,7 @@ struct size against the value the library reports.
 """
 import ctypes as C
 
-NS2D_ABI_VERSION = 1
+NS2D_ABI_VERSION = 2
 
 # ns2d_status
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_NOMEM, ERR_BLOWUP, ERR_DT, ERR_ITERS, ERR_STATE, ERR_NO_DEVICE = range(10)
@@ -21,6 +21,7 @@ RK4CN, RK4, AB4, DP5 = 0, 1, 2, 3
 DEALIAS_23, DEALIAS_HOU_LI = 0, 1
 FORCING_NONE, FORCING_KOLM, FORCING_ZERO = 0, 1, 2
 FP64, FP32 = 0, 1
+MODEL_FULL, MODEL_PHASE_ONLY = 0, 1
 MAX_VORT, MAX_VEL, MAX_VORT_FOUR = 0, 1, 2
 OBJ_ENSTROPHY, OBJ_PALINSTROPHY = 0, 1
 
@@ -45,7 +46,7 @@ class Params(C.Structure):
         ("adapt_step_flag", C.c_int32), ("cfl_cond_flag", C.c_int32),
         ("cfl_const", C.c_double), ("dt", C.c_double),
         ("precision", C.c_int32), ("flux_diagnostics", C.c_int32),
-        ("device", C.c_int32), ("dealias_edge", C.c_int32),
+        ("device", C.c_int32), ("dealias_edge", C.c_int32), ("model", C.c_int32),
     ]
 
     def copy(self):
@@ -112,6 +113,7 @@ def default_params(**kw):
     p.flux_diagnostics = 1
     p.device = 0
     p.dealias_edge = 0
+    p.model = MODEL_FULL
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(f"ns2d_params has no field {k!r}")

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define NS2D_ABI_VERSION 1
+#define NS2D_ABI_VERSION 2
 
 typedef enum ns2d_status {
     NS2D_OK = 0,
@@ -62,6 +62,16 @@ typedef enum ns2d_forcing {
                               single handles only                               */
 } ns2d_forcing;
 typedef enum ns2d_precision { NS2D_FP64 = 0, NS2D_FP32 = 1 } ns2d_precision;
+/* Model type (-D__PHASE_ONLY, data_types.h:75; "PHAEONLY" in the output names,
+   utils.c:515-519).  Phase-only keeps every mode's amplitude through the
+   update of RK4Step (solver.c:634-647, 822-857): after the step each mode
+   k != 0 is rescaled to |w_hat| of the state before it.  RK4CN and RK4 only
+   (AB4Step has no reset, solver.c:261-350; the DP5 path's reset does not
+   compile, solver.c:518-521).  Where the updated mode is exactly 0 (every mode
+   the 2/3 rule zeroes; where the Hou-Li filter underflows, with the
+   reference's integer ratios the corner |kx| = ky = N/2) the reference divides
+   0 by 0 and its step returns NaN there; here the mode stays 0. */
+typedef enum ns2d_model { NS2D_MODEL_FULL = 0, NS2D_MODEL_PHASE_ONLY = 1 } ns2d_model;
 
 /* Reference behaviours that differ from the textbook scheme.  Setting the bit
    reproduces the reference exactly; clearing it gives the corrected form. */
@@ -103,6 +113,7 @@ typedef struct ns2d_params {
                                  1 = zero |k| > (int)(N/3), the post-processing
                                  program's (PostProcessing/src/full_field.c:128);
                                  single handles only                          */
+    int32_t model;            /* ns2d_model; single handles only, RK4CN / RK4     */
 } ns2d_params;
 
 /* Scalars of ComputeSystemMeasurables (Solver/src/sys_msr.c:32-373), in order. */

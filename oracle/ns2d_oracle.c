@@ -313,6 +313,7 @@ void oracle_rk4_step(ns2d_oracle* o, double dt) {
         for (int j = 0; j < o->nyf; ++j) {
             size_t idx = (size_t)i * o->nyf + j;
             if (o->kx[i] != 0 || o->ky[j] != 0) {
+                const double a_before = cabs(o->w_hat[idx]);
                 if (explicit_rk4 || euler) {
                     o->w_hat[idx] = o->w_hat[idx] + (dt / 6.0) * (o->rk[0][idx] + 2.0 * o->rk[1][idx] +
                                                                  2.0 * o->rk[2][idx] + o->rk[3][idx]);
@@ -323,6 +324,10 @@ void oracle_rk4_step(ns2d_oracle* o, double dt) {
                                     (2.0 * dt / (2.0 + D)) * (kB1 * o->rk[0][idx] + kB2 * o->rk[1][idx] +
                                                               kB3 * o->rk[2][idx] + kB4 * o->rk[3][idx]);
                 }
+                /* phase-only amplitude reset (:822-824, 855-857): w *= |w before| / |w after|;
+                   the reference's 0/0 (NaN) where the update gives exactly 0 is kept at 0 */
+                if (o->p.model == NS2D_MODEL_PHASE_ONLY && cabs(o->w_hat[idx]) > 0.0)
+                    o->w_hat[idx] *= (a_before / cabs(o->w_hat[idx]));
             } else {
                 o->w_hat[idx] = 0.0;
             }

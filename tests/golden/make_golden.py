@@ -53,17 +53,44 @@ def cases():
         # ZERO forcing: modes with |kx| <= 2 or |ky| <= 2 killed every step
         "zero32_rk4cn": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, forcing=abi.FORCING_ZERO, force_k=2, dt=1e-3),
                          ("decaying", 9, 6.0), [("steps", 10, 1e-3), ("w_hat",), ("meas",)]),
+        # phase-only model (-D__PHASE_ONLY): amplitudes reset after each update.
+        # The reference's reset divides 0 by 0 wherever the update is exactly 0
+        # (outside the 2/3 disc; the Hou-Li corner kx = ky = N/2); each step here
+        # starts from the previous step's output with those NaN modes set to 0.
+        "po32_rk4cn": ("rk4cn_po", dict(nx=32, ny=32, nu=1e-3, model=abi.MODEL_PHASE_ONLY, dt=1e-3),
+                       ("decaying", 12, 4.0), [("po_steps", 10, 1e-3), ("w_hat",)]),
+        "po32_rk4": ("rk4_po", dict(nx=32, ny=32, nu=1e-3, integrator=abi.RK4, model=abi.MODEL_PHASE_ONLY,
+                                    ekmn_drag_flag=1, dt=1e-3),
+                     ("decaying", 13, 4.0), [("po_steps", 10, 1e-3), ("w_hat",)]),
+        "po32_houli": ("houli_po", dict(nx=32, ny=32, nu=5e-4, dealias=abi.DEALIAS_HOU_LI,
+                                        model=abi.MODEL_PHASE_ONLY, dt=1e-3),
+                       ("decaying", 14, 6.0, None, "houli_ic"), [("po_steps", 10, 1e-3), ("w_hat",)]),
         # adaptive CFL step with the reference's row-index quirk
         "cfl32": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9, dt=1e-3),
                   ("decaying", 6, 4.0), [("cfl", 1e-3), ("steps", 5, 2e-3), ("cfl", 2e-3), ("w_hat",)]),
     }
 
 
+def houli_filter_int(n):
+    """The Hou-Li filter that ends InitialConditions in a Hou-Li build
+    (solver.c:1088, 1994), with its integer ratios k/(N/2): 1 inside, exp(-36)
+    on the Nyquist row and column, 0 (underflow) at their corner."""
+    kx = np.fft.fftfreq(n, 1.0 / n).astype(int)
+    kx[n // 2] = -(n // 2)
+    ky = np.arange(n // 2 + 1)
+    fx = np.trunc(kx / (n // 2))[:, None]
+    fy = np.trunc(ky / (n // 2))[None, :]
+    return np.exp(-36.0 * np.sqrt(fx ** 2 + fy ** 2) ** 36)
+
+
 def make_ic(spec, n):
     if spec[0] == "tg":
         return initial.taylor_green(n)
     if spec[0] == "decaying":
-        return initial.decaying(n, seed=spec[1], k0=spec[2], dealias=spec[3] if len(spec) > 3 else "2/3")
+        w = initial.decaying(n, seed=spec[1], k0=spec[2], dealias=spec[3] if len(spec) > 3 else "2/3")
+        if len(spec) > 4 and spec[4] == "houli_ic":
+            w = w * houli_filter_int(n)
+        return w
     if spec[0] == "noise":
         return initial.noise(n, seed=spec[1], amplitude=1e-3, kolm=True)
     raise ValueError(spec)
@@ -77,6 +104,13 @@ def run_program(solver, w0, program, record):
         if kind == "steps":
             for _ in range(op[1]):
                 solver.rk4_step(op[2])
+        elif kind == "po_steps":
+            for _ in range(op[1]):
+                solver.rk4_step(op[2])
+                w = solver.get_w_hat()
+                if np.isnan(w).any():
+                    w[np.isnan(w)] = 0.0
+                    solver.set_w_hat(w)
         elif kind == "ab4":
             for it in range(1, op[1] + 1):
                 solver.ab4_step(op[2], it)

@@ -313,7 +313,10 @@ def read(path):
 def as_complex(a):
     """Compound {r, i} doubles as complex128."""
     if a.dtype.names and set(a.dtype.names) == {"r", "i"}:
-        return a["r"] + 1j * a["i"]
+        out = np.empty(a.shape, np.complex128)  # part by part: keeps the sign of zero parts
+        out.real = a["r"]
+        out.imag = a["i"]
+        return out
     return a
 
 

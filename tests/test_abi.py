@@ -78,3 +78,19 @@ def test_invalid_sizes_rejected_before_device_use():
         p = abi.default_params(nx=nx, ny=ny)
         h = C.c_void_p()
         assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+
+
+def test_phase_only_combinations_rejected_before_device_use():
+    """The phase-only model is RK4Step's (solver.c:822-857): AB4 and DP5 with
+    it are unsupported; model values other than 0 and 1 are invalid."""
+    L = load()
+    h = C.c_void_p()
+    for integ in (abi.AB4, abi.DP5):
+        p = abi.default_params(integrator=integ, model=abi.MODEL_PHASE_ONLY)
+        assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_UNSUPPORTED
+    for model in (-1, 2):
+        p = abi.default_params(model=model)
+        assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_INVALID
+    p = abi.default_params(model=abi.MODEL_PHASE_ONLY)
+    e = C.c_void_p()
+    assert L.ns2d_ensemble_create(C.byref(p), 1, (C.c_int32 * 1)(64), C.byref(e)) == abi.ERR_UNSUPPORTED

@@ -239,3 +239,56 @@ def test_file_only_output(tmp_path):
     assert names[0].startswith("Main_HDF_Data_SIM[NAV-RK4CN-FULL]_N[64,64]")
     for n in names:
         h5read.read(str(tmp_path / "out" / n))
+
+
+def test_phase_only_matches_reference_program(tmp_path):
+    """--phase-only against the reference program built with -D__PHASE_ONLY
+    (Solver/Makefile:58): the PHAEONLY directory, the a_k / phi_k datasets
+    (the initial save's row-indexed form, hdf5_funcs.c:264-290), and after one
+    step every mode the reference leaves finite.  The reference's reset divides
+    0 by 0 in the modes the 2/3 rule zeroes (NaN there, and everywhere from the
+    next transform on); bin/ns2d keeps them at 0."""
+    exe = REF + "_phase_only"
+    if not os.path.exists(exe):
+        pytest.skip("phase-only reference program not built")
+    args = f"{BASE} -e 0.001 -h 0.001 -p 1 -i DECAY_TURB_BB -o out/"
+    (tmp_path / "ref").mkdir()
+    (tmp_path / "gpu").mkdir()
+    _run(exe, args, tmp_path / "ref")
+    _run(NS2D, args, tmp_path / "gpu", ["--quiet", "--phase-only"])
+    rdirs = sorted(os.listdir(tmp_path / "ref" / "out"))
+    assert rdirs == sorted(os.listdir(tmp_path / "gpu" / "out")) and len(rdirs) == 1
+    assert "_PHAEONLY_" in rdirs[0]
+    want, _, _ = h5log.read(str(tmp_path / "ref" / "out" / rdirs[0] / "Main_HDF_Data.h5"))
+    got, _ = h5read.flatten(h5read.read(str(tmp_path / "gpu" / "out" / rdirs[0] / "Main_HDF_Data.h5")))
+    assert set(got) == set(want) and "/Iter_00001/a_k" in got
+    bad = [k for k in want if k.startswith("/Iter_00000/") and _mismatch(got[k], want[k])]
+    assert not bad, bad
+    nan = np.isnan(want["/Iter_00001/w_hat"])
+    assert nan.any() and not np.isnan(got["/Iter_00001/w_hat"]).any()
+    for name in ("w_hat", "a_k", "phi_k"):
+        g, w = got[f"/Iter_00001/{name}"], want[f"/Iter_00001/{name}"]
+        assert np.all(g[nan] == 0), name
+        assert _mismatch(g[~nan], w[~nan]) is None, name
+    details = (tmp_path / "gpu" / "out" / rdirs[0] / "SimulationDetails.txt").read_text()
+    assert "Model Type: PHAEONLY" in details
+
+
+def test_phase_only_run_keeps_amplitudes(tmp_path):
+    """A longer --phase-only run (corrected conjugacy): finite fields, every
+    save's a_k equal to |w_hat| and to the initial amplitudes."""
+    _run(NS2D, "-n 64 -n 64 -e 0.02 -h 0.001 -p 5 -v 0.001 -i DECAY_TURB_BB -o out/", tmp_path,
+         ["--quiet", "--phase-only", "--no-quirks"])
+    main = glob.glob(str(tmp_path / "out" / "*" / "Main_HDF_Data.h5"))[0]
+    data, _ = h5read.flatten(h5read.read(main))
+    a0 = np.abs(data["/Iter_00000/w_hat"])
+    a0[0, 0] = 0
+    iters = sorted({k.split("/")[1] for k in data})
+    assert len(iters) == 5
+    for it in iters:
+        w = data[f"/{it}/w_hat"]
+        assert np.isfinite(w).all() and np.isfinite(data[f"/{it}/w"]).all()
+        assert np.abs(data[f"/{it}/a_k"] - np.abs(w)).max() <= 1e-15 * a0.max()
+        dphi = data[f"/{it}/phi_k"] - np.angle(w)
+        assert np.abs(dphi).max() <= 1e-14, np.abs(dphi).max()
+        assert np.abs(np.abs(w) - a0).max() <= 1e-12 * a0.max()
