@@ -141,6 +141,11 @@ __device__ __noinline__ Real houli_filter(int kx, int ky, int nx, int ny, int qu
     return (Real)exp(-e);
 }
 
+// Hint that a global line will be read soon (PTX prefetch.global.L2).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Asynchronous global -> shared copies (cp.async, sm_80+ PTX).
 template <typename C>
 __device__ __forceinline__ void cp_async_elem(C* smem, const C* gmem) {
@@ -296,6 +301,14 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 }
             }
             cp_async_commit();
+        }
+        if constexpr (MODE == COL_FINAL) {
+            // the Crank-Nicolson factors are read in the epilogue: start bringing
+            // this thread's entries into L2 now, under the forward transform
+            if (a.cn && valid) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) prefetch_l2(a.cn + (size_t)(t + T * m) * ldc + ky);
+            }
         }
         fft_batched<N, -1, 1>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
         // The epilogue runs as a rolled loop over this thread's elements (one

@@ -85,57 +85,109 @@ def ncu_traffic(cls):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled while the timed steps run.
+
+    The timed region of the default run is tens of milliseconds, shorter than
+    nvidia-smi's 200 ms sampling period, so the clocks are read through NVML
+    (the library nvidia-smi reports from) every 2 ms by a thread; the fields
+    are nvidia-smi's clocks.sm, clocks.max.sm and clocks_event_reasons.*.
+    Without NVML, `nvidia-smi -lms 200` runs instead (and may see no sample
+    inside a short region)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+    SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.sm, self.mx, self.reasons = [], None, set()
+        self.source = None
+        self._stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            prop = torch.cuda.get_device_properties(self.device)
+            bus = f"{prop.pci_domain_id:08X}:{prop.pci_bus_id:02X}:{prop.pci_device_id:02X}.0"
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        return pynvml, h
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self.nvml = self._nvml_handle()
+            self.source = "nvml, 2 ms period"
+            self.t = threading.Thread(target=self._poll, daemon=True)
         except Exception:
-            self.proc = None
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.SMI_FIELDS,
+                                              "--format=csv,noheader,nounits", "-lms", "200", "-i", str(self.device)],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi -lms 200"
+                self.t = threading.Thread(target=self._read, daemon=True)
+            except Exception:
+                self.proc = None
+                return self
+        self.t.start()
         return self
+
+    def _poll(self):
+        pynvml, h = self.nvml
+        bits = [(name, getattr(pynvml, const)) for name, const in self.REASONS]
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.reasons.update(name for name, b in bits if r & b)
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            parts = [p.strip() for p in line.strip().split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                self.sm.append(float(parts[1]))
+                self.mx = float(parts[2])
+            except ValueError:
+                continue
+            for (name, _), v in zip(self.REASONS, parts[5:9]):
+                if v.lower() == "active":
+                    self.reasons.add(name)
 
     def __exit__(self, *exc):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.nvml or self.proc:
+            self.t.join(timeout=5)
+        if self.nvml:
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": self.mx, "reasons": ["unavailable"], "source": self.source}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.mx, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": self.source}
 
 
 def cpu_reference(steps, warmup, threads, budget_s=None):
