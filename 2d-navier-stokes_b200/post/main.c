@@ -38,6 +38,7 @@
 
 #include "ns2d.h"
 #include "ns2d_h5.h"
+#include "phase_sync.h"
 
 #define NUM_K1_SECTORS 8 /* PostProcessing/src/data_types.h:97 */
 
@@ -47,6 +48,7 @@ typedef struct post_args {
     int k3_sectors, k1_sectors, threads, force_k;
     double kmax_frac, nu, hyper_pow, alpha, drag_pow, force_scale;
     int hyper_flag, drag_flag, device;
+    int reduced_k1, phase_sync;
 } post_args;
 
 static void die(const char* msg, double v) {
@@ -83,7 +85,8 @@ static void parse(int argc, char** argv, post_args* a) {
     a->alpha = 0.1;
     a->drag_pow = -2.0;
     int seen_o = 0, seen_i = 0, seen_a = 0, seen_v = 0, seen_d = 0, seen_f = 0, c;
-    static const struct option longs[] = {{"device", required_argument, 0, 1000}, {0, 0, 0, 0}};
+    static const struct option longs[] = {
+        {"device", required_argument, 0, 1000}, {"phase-sync", no_argument, 0, 1001}, {0, 0, 0, 0}};
     optind = 1;
     while ((c = getopt_long(argc, argv, "a:o:h:n:s:e:t:v:i:c:p:f:z:k:t:d:", longs, NULL)) != -1) {
         switch (c) {
@@ -102,8 +105,10 @@ static void parse(int argc, char** argv, post_args* a) {
                 } else if (seen_a == 1) {
                     a->k1_sectors = atoi(optarg);
                     if (a->k1_sectors <= 0) die("The number of sectors [%g] must be positive", a->k1_sectors);
-                } else {
+                } else if (seen_a == 2) {
+                    /* reduced k1 search (utils.c:128-133) */
                     a->k1_sectors = NUM_K1_SECTORS;
+                    a->reduced_k1 = 1;
                 }
                 seen_a++;
                 break;
@@ -156,6 +161,10 @@ static void parse(int argc, char** argv, post_args* a) {
                 break;
             case 1000:
                 a->device = atoi(optarg);
+                break;
+            case 1001:
+                /* the -D__SEC_PHASE_SYNC build (PostProcessing/src/data_types.h:62) */
+                a->phase_sync = 1;
                 break;
             default:
                 fprintf(stderr, "\n[ERROR] Incorrect command line flag encountered\n\nExample usage:\n\tns2d_post -i "
@@ -312,6 +321,17 @@ int main(int argc, char** argv) {
         fprintf(stderr, "out of memory\n");
         return 1;
     }
+    ps_state* ps = NULL;
+    double complex* rhs = NULL;
+    if (a.phase_sync) {
+        ps = ps_create((int)nx, kmax, a.kmax_frac, a.k3_sectors, a.k1_sectors, a.reduced_k1, a.nu, a.hyper_flag,
+                       a.hyper_pow, a.alpha, a.drag_flag, a.drag_pow, a.device);
+        rhs = (double complex*)malloc(sizeof(double complex) * (size_t)(nx * nyf));
+        if (!ps || !rhs) {
+            fprintf(stderr, "out of memory\n");
+            return 1;
+        }
+    }
     ns2d_h5_file* f = ns2d_h5_create(out_file);
     h5die(f ? 0 : -1, NULL, out_file);
     /* dataset order of WriteDataToFile (hdf5_funcs.c:524-790); spectra index
@@ -357,6 +377,12 @@ int main(int argc, char** argv) {
             snprintf(path, sizeof(path), "%s/%s", sg, sp_names[k]);
             h5die(ns2d_h5_dataset(f, path, NS2D_H5_F64, 1, dsp, spec + (size_t)sp_index[k] * n_spec), f, path);
         }
+        if (ps) {
+            /* FluxSpectra's sector sums and PhaseSyncSector (post_proc.c:88-104) */
+            check(ns2d_nonlinear_rhs(g_h, (const double*)w, (double*)rhs), "NonlinearRHS");
+            check(ps_snapshot(ps, w, rhs, ff + w2, ff), "phase sync");
+            h5die(ps_write_snapshot(ps, f, sg), f, sg);
+        }
         printf("Snapshot: %d\n", s);
     }
     /* FinalWriteAndClose (hdf5_funcs.c:1290-1370) */
@@ -380,10 +406,13 @@ int main(int argc, char** argv) {
     h5die(ns2d_h5_dataset(f, "Time", NS2D_H5_F64, 1, ds, tvals), f, "Time");
     static const char* const c_names[4] = {"EnstrophyFluxC", "EnstrophyDissC", "EnergyFluxC", "EnergyDissC"};
     for (int k = 0; k < 4; ++k) h5die(ns2d_h5_dataset(f, c_names[k], NS2D_H5_F64, 1, ds, csum + (size_t)k * snaps), f, c_names[k]);
+    if (ps) h5die(ps_write_final(ps, f), f, "phase sync");
     h5die(ns2d_h5_close(f), NULL, out_file);
     const double secs = (double)(clock() - begin) / CLOCKS_PER_SEC;
     printf("\n\nTotal Execution Time: [%5.10lf]\n\n", secs);
     ns2d_destroy(g_h);
+    ps_free(ps);
+    free(rhs);
     free(w);
     free(spec);
     free(ff);

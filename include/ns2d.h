@@ -273,6 +273,43 @@ ns2d_status ns2d_mean_flow(ns2d_handle* h, double* mean_x, double* mean_y);
 ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const double* d_w_hat, double* d_rhs,
                                        void* cuda_stream);
 
+/* ---- Sector triad sums (post-processing phase synchronisation) -------------
+   One snapshot's sums of PhaseSyncSector (PostProcessing/src/phase_sync.c:
+   281-1058) over the triads (k1, k2 = k3 - k1, k3) of its sector search
+   (AllocatePhaseSyncMemory, phase_sync.c:1744-1948), without storing the
+   triads: the caller passes the sector bounds and the wavevector angles it
+   computed, and the snapshot's amplitudes and phases in the full-field layout
+   of FullFieldData (index (kmax - kx)(2 kmax + 1) + kmax + ky, |kx|, |ky| <=
+   kmax).  The sums come back per class
+
+     sums[((((a n_k1 + l) 2 + term) 3 + cls) 2 + contrib) 2 + unidir][8]
+
+   with a the k3 sector, l the k1 sector as stored (phase_sync.c:1776),
+   term 0 the positive flux term and 1 the negative one, cls the sign of
+   flux_pre_fac (0: < 0, 1: > 0, 2: == 0), contrib 0 / 1 for 1d / 2d
+   contributions and unidir the unidirectional condition of C_theta (k3_y >= 0
+   for the positive term, k1_y >= 0 and k2_y >= 0 for the negative); the eight
+   values are the triad count, the enstrophy flux (sign of the term applied),
+   sum exp(i phi) of the generalised phase of type 0, the same for the triad's
+   own type (they differ for cls 2 of the negative term), and the collective
+   term's sum (re, im).  Host arrays; one call allocates, runs and frees on
+   `device`. */
+#define NS2D_TRIAD_VALUES 8
+typedef struct ns2d_triad_sectors {
+    int32_t kmax;               /* tables cover |kx|, |ky| <= kmax                  */
+    int32_t n_k3, n_k1;         /* sector counts                                   */
+    int32_t reserved;
+    double kmax_sqr, kmax_c_sqr;/* kmax^2 (<= kmax * kmax) and kmax_C^2             */
+    const double* k3_lwr;       /* [n_k3] sector bounds theta_k3 -+ dtheta_k3 / 2   */
+    const double* k3_upr;
+    const double* k1_lwr;       /* [n_k3 * n_k1] bounds of the k1 sector stored at (a, l) */
+    const double* k1_upr;
+    const double* angle;        /* [(2kmax+1)^2] atan2(kx, ky)                      */
+    const double* angle_neg;    /* [(2kmax+1)^2] atan2(-kx, -ky)                    */
+} ns2d_triad_sectors;
+ns2d_status ns2d_triad_sector_sums(int32_t device, const ns2d_triad_sectors* g, const double* amps,
+                                   const double* phases, double* sums);
+
 /* ---- Discrete adjoint ------------------------------------------------------
    Gradient of a final-time functional J(w(T)) with respect to the initial
    vorticity for n fixed-dt RK4CN steps (RK4Step, solver.c:625-873, over

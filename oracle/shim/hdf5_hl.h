@@ -4,4 +4,5 @@
 #include "hdf5.h"
 herr_t H5LTmake_dataset(hid_t loc, const char* name, int rank, const hsize_t* dims, hid_t type, const void* buf);
 herr_t H5LTread_dataset_double(hid_t loc, const char* name, double* buf);
+herr_t H5LTread_dataset(hid_t loc, const char* name, hid_t type, void* buf);
 #endif
