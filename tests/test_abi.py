@@ -94,3 +94,28 @@ def test_phase_only_combinations_rejected_before_device_use():
     p = abi.default_params(model=abi.MODEL_PHASE_ONLY)
     e = C.c_void_p()
     assert L.ns2d_ensemble_create(C.byref(p), 1, (C.c_int32 * 1)(64), C.byref(e)) == abi.ERR_UNSUPPORTED
+
+
+def test_triad_sector_sums_rejects_bad_arguments_before_device_use():
+    """ns2d_triad_sector_sums validates its geometry before touching a device:
+    missing tables or a kmax_sqr that would let k2 leave the tables are
+    invalid."""
+    L = load()
+
+    class Geo(C.Structure):
+        _fields_ = [("kmax", C.c_int32), ("n_k3", C.c_int32), ("n_k1", C.c_int32), ("reserved", C.c_int32),
+                    ("kmax_sqr", C.c_double), ("kmax_c_sqr", C.c_double)] + [
+                       (n, C.POINTER(C.c_double)) for n in ("k3_lwr", "k3_upr", "k1_lwr", "k1_upr", "angle", "angle_neg")]
+
+    buf = (C.c_double * 1024)()
+    p = C.cast(buf, C.POINTER(C.c_double))
+    g = Geo(kmax=5, n_k3=2, n_k1=2, kmax_sqr=25.0, kmax_c_sqr=4.0, k3_lwr=p, k3_upr=p, k1_lwr=p, k1_upr=p,
+            angle=p, angle_neg=p)
+    L.ns2d_triad_sector_sums.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    bad = Geo.from_buffer_copy(g)
+    bad.kmax_sqr = 26.0
+    assert L.ns2d_triad_sector_sums(0, C.byref(bad), buf, buf, buf) == abi.ERR_INVALID
+    bad = Geo.from_buffer_copy(g)
+    bad.angle = None
+    assert L.ns2d_triad_sector_sums(0, C.byref(bad), buf, buf, buf) == abi.ERR_INVALID
+    assert L.ns2d_triad_sector_sums(0, C.byref(g), None, buf, buf) == abi.ERR_INVALID
