@@ -25,6 +25,7 @@ struct TriadArgs {
     const double *k3_lwr, *k3_upr, *k1_lwr, *k1_upr;
     const double *ang, *ang_neg, *amps, *phases;
     double* sums;
+    int use_list;  // compact the block's k1 candidates into shared memory first
 };
 
 // ((angle in [lo, hi)) or (angle of -k in [lo, hi))), as the search tests a sector
@@ -58,6 +59,45 @@ __global__ void __launch_bounds__(kThreads) triad_sector_kernel(TriadArgs g) {
 #pragma unroll
         for (int v = 0; v < kVals; ++v) acc[s][v] = 0.0;
 
+    // k1 candidates of this block's sectors and term, compacted in order into
+    // shared memory (index | 1d flag << 30): the k1-only tests of the search
+    // run once per block instead of once per selected k3
+    extern __shared__ int k1_list[];
+    __shared__ int warp_count[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int n1 = m;
+    if (g.use_list) {
+        n1 = 0;
+        for (int base = 0; base < m; base += kThreads) {
+            const int i1 = base + (int)threadIdx.x;
+            int code = -1;
+            if (i1 < m) {
+                const int k1x = g.kmax - i1 / side, k1y = i1 % side - g.kmax;
+                const double k1s = (double)(k1x * k1x + k1y * k1y);
+                const double a1 = g.ang[i1], n1a = g.ang_neg[i1];
+                const bool s13 = in_sector(a1, n1a, lo3, hi3), s11 = in_sector(a1, n1a, lo1, hi1);
+                if (term == 0) {
+                    const bool c1d = (k1s > 0.0 && k1s <= kc) && s13 && s11;
+                    const bool c2d = (k1s > 0.0 && k1s <= km) && s11 && !s13;
+                    if (c1d || c2d) code = i1 | (c1d ? (1 << 30) : 0);
+                } else if ((k1s > kc && k1s <= km) && s13) {
+                    code = i1;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, code >= 0);
+            if (lane == 0) warp_count[warp] = __popc(bal);
+            __syncthreads();
+            int off = n1, tot = 0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                if (w < warp) off += warp_count[w];
+                tot += warp_count[w];
+            }
+            if (code >= 0) k1_list[off + __popc(bal & ((1u << lane) - 1u))] = code;
+            __syncthreads();
+            n1 += tot;
+        }
+    }
+
     for (int i3 = 0; i3 < m; ++i3) {
         // table index (kmax - kx) * side + kmax + ky (the full-field layout)
         const int k3x = g.kmax - i3 / side, k3y = i3 % side - g.kmax;
@@ -71,21 +111,30 @@ __global__ void __launch_bounds__(kThreads) triad_sector_kernel(TriadArgs g) {
         const bool neg = !pos && (neg_2d || neg_1d);
         if (term == 0 ? !pos : !neg) continue;
         const double amp3 = g.amps[i3], ph3 = g.phases[i3];
-        for (int i1 = threadIdx.x; i1 < m; i1 += kThreads) {
+        for (int j = threadIdx.x; j < n1; j += kThreads) {
+            int i1, contrib;
+            if (g.use_list) {
+                const int code = k1_list[j];
+                i1 = code & ((1 << 30) - 1);
+                contrib = term == 0 ? ((code >> 30) ? 0 : 1) : (neg_1d ? 0 : 1);
+            } else {
+                i1 = j;
+                const int kx = g.kmax - i1 / side, ky = i1 % side - g.kmax;
+                const double ks = (double)(kx * kx + ky * ky);
+                const double a1 = g.ang[i1], n1a = g.ang_neg[i1];
+                const bool s13 = in_sector(a1, n1a, lo3, hi3), s11 = in_sector(a1, n1a, lo1, hi1);
+                if (term == 0) {
+                    const bool c1d = (ks > 0.0 && ks <= kc) && s13 && s11;
+                    const bool c2d = (ks > 0.0 && ks <= km) && s11 && !s13;
+                    if (!(c1d || c2d)) continue;
+                    contrib = c1d ? 0 : 1;
+                } else {
+                    if (!((ks > kc && ks <= km) && s13)) continue;
+                    contrib = neg_1d ? 0 : 1;
+                }
+            }
             const int k1x = g.kmax - i1 / side, k1y = i1 % side - g.kmax;
             const double k1s = (double)(k1x * k1x + k1y * k1y);
-            const double a1 = g.ang[i1], n1 = g.ang_neg[i1];
-            const bool s13 = in_sector(a1, n1, lo3, hi3), s11 = in_sector(a1, n1, lo1, hi1);
-            int contrib;
-            if (term == 0) {
-                const bool c1d = (k1s > 0.0 && k1s <= kc) && s13 && s11;
-                const bool c2d = (k1s > 0.0 && k1s <= km) && s11 && !s13;
-                if (!(c1d || c2d)) continue;
-                contrib = c1d ? 0 : 1;
-            } else {
-                if (!((k1s > kc && k1s <= km) && s13)) continue;
-                contrib = neg_1d ? 0 : 1;
-            }
             const int k2x = k3x - k1x, k2y = k3y - k1y;
             const double k2s = (double)(k2x * k2x + k2y * k2y);
             if (term == 0) {
@@ -135,7 +184,6 @@ __global__ void __launch_bounds__(kThreads) triad_sector_kernel(TriadArgs g) {
 
     // block sums in a fixed order: warps by shuffle, then the warps in turn
     __shared__ double part[kThreads / 32][kSub * kVals];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int s = 0; s < kSub; ++s)
 #pragma unroll
@@ -208,7 +256,14 @@ extern "C" ns2d_status ns2d_triad_sector_sums(int32_t device, const ns2d_triad_s
     args.k1_lwr = db + 2 * g->n_k3;
     args.k1_upr = db + 2 * g->n_k3 + nal;
     args.sums = d + (ndbl - nsum);
-    triad_sector_kernel<<<dim3((unsigned)nal, 6), kThreads>>>(args);
+    // the compacted k1 list in shared memory (up to kmax = 112)
+    const size_t list_bytes = sizeof(int) * m;
+    args.use_list = list_bytes <= 200 * 1024 ? 1 : 0;
+    const size_t smem = args.use_list ? list_bytes : 0;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(triad_sector_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return NS2D_ERR_CUDA;
+    triad_sector_kernel<<<dim3((unsigned)nal, 6), kThreads, smem>>>(args);
     if (cudaGetLastError() != cudaSuccess) return NS2D_ERR_CUDA;
     if (cudaMemcpy(sums, args.sums, sizeof(double) * nsum, cudaMemcpyDeviceToHost) != cudaSuccess) return NS2D_ERR_CUDA;
     return NS2D_OK;
