@@ -6,6 +6,8 @@ per-snapshot dataset and the set-C sums agree to 1e-10 of their scale (the
 scale floor of test_gpu_cli.py for quantities that vanish up to rounding).
 256^2 runs put modes on the dealiasing circle |k| = N/3, where the
 post-processing program's edge (|k| > N/3 zeroed) differs from the solver's.
+--phase-sync is checked against that program's phase_sync.c (-D__SEC_PHASE_SYNC)
+behind oracle/phase_sync_harness.c.
 """
 import ctypes as C
 import glob
