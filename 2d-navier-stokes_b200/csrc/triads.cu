@@ -208,6 +208,15 @@ struct DevBuf {
     }
 };
 
+// Restores the calling thread's current device on return.
+struct DeviceScope {
+    int prev = -1;
+    DeviceScope() { cudaGetDevice(&prev); }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" ns2d_status ns2d_triad_sector_sums(int32_t device, const ns2d_triad_sectors* g, const double* amps,
@@ -220,13 +229,15 @@ extern "C" ns2d_status ns2d_triad_sector_sums(int32_t device, const ns2d_triad_s
     if ((long long)g->n_k3 * g->n_k1 > 65535) return NS2D_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NS2D_ERR_NO_DEVICE;
-    if (device < 0 || device >= ndev || cudaSetDevice(device) != cudaSuccess) return NS2D_ERR_INVALID;
+    if (device < 0 || device >= ndev) return NS2D_ERR_INVALID;
+    DeviceScope scope;
+    if (cudaSetDevice(device) != cudaSuccess) return NS2D_ERR_INVALID;
+    DevBuf buf;  // released before the device is restored
     const size_t side = 2 * (size_t)g->kmax + 1, m = side * side;
     const size_t nal = (size_t)g->n_k3 * g->n_k1;
     const size_t nsum = nal * 6 * kSub * kVals;
     // one buffer: tables (4 m), sector bounds (2 n_k3 + 2 nal), sums
     const size_t ndbl = 4 * m + 2 * (size_t)g->n_k3 + 2 * nal + nsum;
-    DevBuf buf;
     if (cudaMalloc(&buf.p, sizeof(double) * ndbl) != cudaSuccess) return NS2D_ERR_NOMEM;
     double* d = (double*)buf.p;
     std::vector<double> host(ndbl - nsum);
