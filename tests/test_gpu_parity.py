@@ -78,6 +78,26 @@ def test_rhs_every_grid_size(n):
     s.close()
 
 
+@pytest.mark.parametrize("integ", [abi.RK4CN, abi.RK4])
+@pytest.mark.parametrize("n", [16, 2048])
+def test_steps_at_grid_size_limits(n, integ):
+    """The smallest and largest grids ns2d_create takes: three steps equal the
+    oracle's (the per-call step, then the graph-replayed form)."""
+    dt = 1e-3 if n == 16 else 1e-4
+    p = abi.default_params(nx=n, ny=n, nu=1e-3, integrator=integ, ekmn_drag_flag=1, dt=dt)
+    w0 = initial.decaying(n, seed=300 + n, k0=min(6.0, n / 8), dealias="2/3")
+    o = Oracle(p, threads=8)
+    o.set_w_hat(w0)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    for _ in range(3):
+        o.rk4_step(dt)
+    s.rk4_step(dt)
+    s.step_n(2, dt)
+    assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-12, (n, integ)
+    s.close()
+
+
 def test_kolmogorov_1024_fp64_steps():
     """BASELINE config 3 (FP64): Kolmogorov n = 4, F = 1, nu = 1e-4 plus
     hyperviscosity nu_h k^16 through the RK4CN drag branch, dt = 2.5e-4."""
