@@ -172,6 +172,7 @@ ns2d_status create_t(ns2d_ensemble* e) {
         a.norm2 = (Real)std::pow(1.0 / (double)(n * n), 2.0);
         a.inv_nxny = 1.0 / (double)(n * n);
         a.cn = (const double2*)cn;
+        a.phase_only = e->p.model == NS2D_MODEL_PHASE_ONLY ? 1 : 0;
         mb.row.f0 = (const C*)f[0];
         mb.row.f1 = (const C*)f[1];
         mb.row.f2 = (const C*)f[2];
@@ -439,7 +440,7 @@ ns2d_status ns2d_ensemble_create(const ns2d_params* base, int32_t n_members, con
     if (base->integrator != NS2D_RK4CN && base->integrator != NS2D_RK4) return NS2D_ERR_UNSUPPORTED;
     if (base->forcing == NS2D_FORCING_ZERO) return NS2D_ERR_UNSUPPORTED;  // mode killing: single handles only
     if (base->dealias_edge != 0) return NS2D_ERR_UNSUPPORTED;            // the solver's 2/3 edge only
-    if (base->model != NS2D_MODEL_FULL) return NS2D_ERR_UNSUPPORTED;     // phase-only: single handles
+    if (base->model != NS2D_MODEL_FULL && base->model != NS2D_MODEL_PHASE_ONLY) return NS2D_ERR_INVALID;
     if (base->precision != NS2D_FP64 && base->precision != NS2D_FP32) return NS2D_ERR_INVALID;
     for (int m = 0; m < n_members; ++m)
         if (!ens_size_ok(sizes[m])) return NS2D_ERR_UNSUPPORTED;

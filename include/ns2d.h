@@ -113,7 +113,7 @@ typedef struct ns2d_params {
                                  1 = zero |k| > (int)(N/3), the post-processing
                                  program's (PostProcessing/src/full_field.c:128);
                                  single handles only                          */
-    int32_t model;            /* ns2d_model; single handles only, RK4CN / RK4     */
+    int32_t model;            /* ns2d_model; RK4CN / RK4 (handles and ensembles)  */
 } ns2d_params;
 
 /* Scalars of ComputeSystemMeasurables (Solver/src/sys_msr.c:32-373), in order. */

@@ -91,9 +91,9 @@ def test_phase_only_combinations_rejected_before_device_use():
     for model in (-1, 2):
         p = abi.default_params(model=model)
         assert L.ns2d_create(C.byref(p), C.byref(h)) == abi.ERR_INVALID
-    p = abi.default_params(model=abi.MODEL_PHASE_ONLY)
+    p = abi.default_params(model=2)
     e = C.c_void_p()
-    assert L.ns2d_ensemble_create(C.byref(p), 1, (C.c_int32 * 1)(64), C.byref(e)) == abi.ERR_UNSUPPORTED
+    assert L.ns2d_ensemble_create(C.byref(p), 1, (C.c_int32 * 1)(64), C.byref(e)) == abi.ERR_INVALID
 
 
 def test_triad_sector_sums_rejects_bad_arguments_before_device_use():

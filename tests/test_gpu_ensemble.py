@@ -38,6 +38,25 @@ def test_fp64_ensemble_equals_single_handles():
     e.close()
 
 
+def test_phase_only_ensemble_equals_single_handles():
+    """The phase-only model (RK4Step's amplitude reset) in an FP64 ensemble
+    of mixed sizes equals single phase-only handles."""
+    sizes = [64, 128, 256]
+    p = abi.default_params(nu=1e-3, dt=1e-3, model=abi.MODEL_PHASE_ONLY)
+    ics = _ics(sizes, seed0=40)
+    e = Ensemble(p, sizes)
+    for m, w in enumerate(ics):
+        e.set_w_hat(m, w)
+    e.step_n(10, 1e-3)
+    for m, n in enumerate(sizes):
+        s = Solver(abi.default_params(nx=n, ny=n, nu=1e-3, dt=1e-3, model=abi.MODEL_PHASE_ONLY))
+        s.set_w_hat(ics[m])
+        s.step_n(10, 1e-3)
+        assert rel_err(e.get_w_hat(m), s.get_w_hat()) <= 1e-14, (m, n)
+        s.close()
+    e.close()
+
+
 def test_fp32_ensemble_enstrophy_vs_fp64_oracle():
     sizes = [128, 256, 128]
     p = abi.default_params(nu=1e-3, dt=1e-3, precision=abi.FP32)
