@@ -159,14 +159,16 @@ np.savez(out, **{k.replace("/", "|"): v for k, v in res.items()})
 
 
 @pytest.mark.skipif(not os.path.exists(PS_HARNESS), reason="phase-sync harness not built (oracle/Makefile cli)")
-@pytest.mark.parametrize("n,kfrac,sectors", [(32, 0.5, []), (64, 0.6, ["-a", "12"]), (32, 0.4, ["-a", "12", "-a", "8", "-a", "x"])])
+@pytest.mark.parametrize("n,kfrac,sectors", [(32, 0.5, []), (64, 0.6, ["-a", "12"]), (32, 0.4, ["-a", "12", "-a", "8", "-a", "x"]),
+                                             (32, 0.5, ["-a", "12", "-a", "1"])])
 def test_phase_sync_matches_reference(n, kfrac, sectors, tmp_path):
     """bin/ns2d_post --phase-sync (triad sums on the GPU) against the reference
     post-processing program's phase_sync.c and the -D__SEC_PHASE_SYNC parts of
     full_field.c on the same snapshots: triad counts equal, per-sector fluxes
     and collective sums to 1e-10 of their scale, order parameters to 1e-10
     (average angles where the order parameter exceeds 1e-6); default sectors,
-    a full 12 x 12 search, and the reduced 8-sector k1 search."""
+    a full 12 x 12 search, the reduced 8-sector k1 search, and one k1 sector
+    (k1 anywhere, phase_sync.c:1762-1766)."""
     _run([NS2D, "--quiet", "-n", str(n), "-n", str(n), "-e", "0.002", "-h", "0.001", "-p", "1", "-v", "0.001",
           "-i", "DECAY_TURB_BB", "-o", "run/"], tmp_path)
     run_dir = os.path.join(glob.glob(str(tmp_path / "run" / "*"))[0], "")
