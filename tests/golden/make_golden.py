@@ -62,6 +62,9 @@ def cases():
         "po32_rk4": ("rk4_po", dict(nx=32, ny=32, nu=1e-3, integrator=abi.RK4, model=abi.MODEL_PHASE_ONLY,
                                     ekmn_drag_flag=1, dt=1e-3),
                      ("decaying", 13, 4.0), [("po_steps", 10, 1e-3), ("w_hat",)]),
+        "po32_kolm": ("rk4cn_po", dict(nx=32, ny=32, nu=1e-3, model=abi.MODEL_PHASE_ONLY, forcing=abi.FORCING_KOLM,
+                                       force_k=4, force_scale=1.0, ekmn_drag_flag=1, ekmn_alpha=0.05, dt=1e-3),
+                      ("decaying", 15, 4.0), [("po_steps", 10, 1e-3), ("w_hat",), ("meas",)]),
         "po32_houli": ("houli_po", dict(nx=32, ny=32, nu=5e-4, dealias=abi.DEALIAS_HOU_LI,
                                         model=abi.MODEL_PHASE_ONLY, dt=1e-3),
                        ("decaying", 14, 6.0, None, "houli_ic"), [("po_steps", 10, 1e-3), ("w_hat",)]),
