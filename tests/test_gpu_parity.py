@@ -120,6 +120,38 @@ def test_kolmogorov_1024_fp64_steps():
     s.close()
 
 
+@pytest.mark.parametrize("integ,order,quirks,nu,sizes", [(abi.RK4CN, 2, abi.QUIRKS_REFERENCE, 0.5, (32, 128)),
+                                                        (abi.RK4, 4, 0, 1.25, (16, 32))])
+def test_taylor_green_time_convergence(integ, order, quirks, nu, sizes):
+    """The reference's convergence study (error_testing.py:105-250, the
+    Taylor-Green test of solver.c:2497-2597) as a check with thresholds: the
+    Taylor-Green vortex, whose nonlinear term vanishes, under nu |k|^2
+    (EKMN_DRAG_FLAG = 1, alpha = 0) decays as exp(-2 nu t); halving dt divides
+    the error at t = 0.4 by 2^order (Crank-Nicolson 2, explicit RK4 4 in its
+    corrected form) and the error does not depend on the grid.  The explicit
+    scheme is stable only for dt nu |k|^2 < 2.78 on every mode the 2/3 rule
+    keeps (the rounding noise there grows otherwise), hence its small grids."""
+    T = 0.4
+    errs = {}
+    for n in sizes:
+        for dt in (0.02, 0.01, 0.005):
+            p = abi.default_params(nx=n, ny=n, nu=nu, ekmn_drag_flag=1, ekmn_alpha=0.0, integrator=integ,
+                                   quirks=quirks, dt=dt)
+            w0 = initial.taylor_green(n)
+            s = Solver(p)
+            s.set_w_hat(w0)
+            s.step_n(int(round(T / dt)), dt)
+            w = s.get_w_hat()
+            s.close()
+            errs[n, dt] = np.abs(w - w0 * np.exp(-2.0 * nu * T)).max() / np.abs(w0).max()
+    for n in sizes:
+        r1 = errs[n, 0.02] / errs[n, 0.01]
+        r2 = errs[n, 0.01] / errs[n, 0.005]
+        assert abs(np.log2(r1) - order) < 0.2 and abs(np.log2(r2) - order) < 0.2, (n, r1, r2, errs)
+    for dt in (0.02, 0.01, 0.005):
+        assert abs(errs[sizes[0], dt] - errs[sizes[1], dt]) <= 1e-3 * errs[sizes[0], dt] + 1e-14
+
+
 def test_decaying_256_houli_cfl():
     """BASELINE config 2 shape: 256^2, nu = 5e-4, Hou-Li filter (reference's
     integer form), CFL 0.9 adaptive step; 20 steps with dt from GetTimestep."""
