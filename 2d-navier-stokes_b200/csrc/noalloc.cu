@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -101,16 +102,31 @@ ns2d_status setup(int dev, int n, double2** base) {
 extern "C" ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const double* d_w_hat, double* d_rhs,
                                                   void* cuda_stream) {
     if (!p || !d_w_hat || !d_rhs) return NS2D_ERR_INVALID;
+    // The kernels move the arrays in 16-byte units (cp.async and double2
+    // stores): an array that starts off that boundary, a float64 view offset
+    // by one element for instance, would raise a misaligned-address error,
+    // which poisons the caller's whole CUDA context.  Refuse it instead.
+    if (((uintptr_t)d_w_hat | (uintptr_t)d_rhs) & 15u) return NS2D_ERR_INVALID;
     const int n = p->nx;
     if (p->nx != p->ny || size_slot(n) < 0 || (size_t)n > kMaxN) return NS2D_ERR_UNSUPPORTED;
-    if (p->precision != NS2D_FP64 || p->dealias < 0 || p->dealias > 1) return NS2D_ERR_INVALID;
+    // the parameter checks of ns2d_create that bear on the nonlinear term
+    if (p->precision != NS2D_FP64 || p->dealias < 0 || p->dealias > 1 || p->dealias_edge < 0 ||
+        p->dealias_edge > 1 || p->forcing < 0 || p->forcing > 2 || p->integrator < 0 || p->integrator > 3 ||
+        p->model < 0 || p->model > 1)
+        return NS2D_ERR_INVALID;
+    const int nyf = n / 2 + 1;
+    if (p->forcing == NS2D_FORCING_KOLM && (p->force_k < 0 || p->force_k / nyf >= n)) return NS2D_ERR_INVALID;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return NS2D_ERR_NO_DEVICE;
+    // the work runs on the current device, which p->device must name
+    if (p->device != dev) return NS2D_ERR_INVALID;
+    // an error left by the caller's own earlier launches stays the caller's:
+    // report it without clearing it, and launch nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return NS2D_ERR_CUDA;
     double2* base = nullptr;
     ns2d_status s = setup(dev, n, &base);
     if (s != NS2D_OK) return s;
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    const int nyf = n / 2 + 1;
     const size_t fe = (size_t)n * nyf;
     double2* f[4] = {base, base + fe, base + 2 * fe, base + 3 * fe};
     double2* nl = base + 4 * fe;
@@ -159,6 +175,7 @@ extern "C" ns2d_status ns2d_nonlinear_rhs_noalloc(const ns2d_params* p, const do
     a.rhs_store = (double2*)d_rhs;  // no state here: the conjugacy side effect is not applied
     a.conj_mode = 0;
     with_small_size(n, [&](auto L) { decltype(L)::col(COL_RHS, a, st); });
+    // no error was pending on entry, so one found now is a launch of this call
     if (cudaGetLastError() != cudaSuccess) return NS2D_ERR_CUDA;
     return NS2D_OK;
 }

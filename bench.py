@@ -235,7 +235,7 @@ ENS_DT = 1e-3
 
 
 def ensemble_bench(stream, flush, steps, warmup, rank):
-    """64 members (32 x 128^2, 24 x 256^2, 8 x 512^2), FP32
+    """The uneven-ensemble workload: 64 members (32 x 128^2, 24 x 256^2, 8 x 512^2), FP32
     RK4CN, nu = 1e-3, decaying spectra with k0 drawn from {4, 6, 8}; every pass
     of a step is one launch for all members, the step replayed from a CUDA
     graph, persistent grids picked by the autotuner.  Returns ensemble steps/s

@@ -256,7 +256,12 @@ ns2d_status ns2d_mean_flow(ns2d_handle* h, double* mean_x, double* mean_y);
    synchronisation, and for applications whose device memory comes from their
    own pool.  No handle: the caller passes the parameters and two device arrays
    in the reference layout, [nx][ny/2+1] complex128 (d_w_hat read, d_rhs
-   written), and the work is queued on cuda_stream (NULL = legacy default).
+   written), both starting on a 16-byte boundary (else NS2D_ERR_INVALID, with
+   nothing launched), and the work is queued on cuda_stream (NULL = legacy
+   default) of the current device, which p->device must name.  The parameters
+   pass ns2d_create's checks or the call returns NS2D_ERR_INVALID.  An error
+   already pending from the caller's earlier launches is reported as
+   NS2D_ERR_CUDA and left pending; nothing is launched then.
    The output equals ns2d_nonlinear_rhs(h, w_hat, rhs) after
    ns2d_compute_forcing on a handle with the same parameters; the conjugacy
    side effect on a state does not apply (there is none).  FP64 only.

@@ -638,7 +638,7 @@ void oracle_system_measurables(ns2d_oracle* o, double* s13, double* spectra) {
     memcpy(s13, out, sizeof out);
 }
 
-/* Taylor-Green test input w = 2 sin x sin y, transformed
+/* Taylor-Green test input w = 2 sin x sin y (the 64^2 Taylor-Green workload), transformed
    with the oracle FFT: w_hat(+-1, 1) = -Nx*Ny/2 * (+-1). */
 void oracle_ic_taylor_green(int nx, int ny, double* w_hat) {
     const int nyf = ny / 2 + 1;

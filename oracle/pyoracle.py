@@ -30,12 +30,10 @@ def _ptr(a):
 
 
 def build(ref=True):
-    """Build the restatement (always) and the reference libraries (when the
-    reference sources are present)."""
-    targets = ["restatement"]
-    if ref and os.path.isdir("/root/reference/Solver/src"):
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    """Build the restatement (always) and, with ref, the reference builds
+    (when the reference sources are present: oracle/Makefile target
+    `checkers`, which reads their location from NS2D_REFERENCE)."""
+    subprocess.run(["make", "-s", "-C", HERE, "checkers" if ref else "restatement"], check=True)
 
 
 def ref_available(variant="rk4cn"):

@@ -23,7 +23,7 @@ from ns2d import abi, initial  # noqa: E402
 def cases():
     """name -> (variant, params kwargs, initial condition spec, program)."""
     return {
-        # BASELINE config 1 shape: Taylor-Green, nu|k|^2 via the drag-flag recipe
+        # the 64^2 Taylor-Green workload: Taylor-Green, nu|k|^2 via the drag-flag recipe
         # of InitFiles/TaylorGreen/tg.ini (EKMN_DRAG_FLAG = 1, alpha = 0).
         "tg64_rk4cn": ("rk4cn", dict(nx=64, ny=64, nu=0.01, ekmn_drag_flag=1, ekmn_alpha=0.0, dt=1e-3),
                        ("tg",), [("steps", 100, 1e-3), ("w_hat",), ("max", 0), ("meas",)]),

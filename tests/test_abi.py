@@ -119,3 +119,26 @@ def test_triad_sector_sums_rejects_bad_arguments_before_device_use():
     bad.angle = None
     assert L.ns2d_triad_sector_sums(0, C.byref(bad), buf, buf, buf) == abi.ERR_INVALID
     assert L.ns2d_triad_sector_sums(0, C.byref(g), None, buf, buf) == abi.ERR_INVALID
+
+
+def test_noalloc_rhs_argument_checks_before_device_use():
+    """ns2d_nonlinear_rhs_noalloc refuses misaligned arrays and parameter sets
+    that ns2d_create refuses before it touches a device (the pointers here are
+    never dereferenced)."""
+    L = load()
+    f = L.ns2d_nonlinear_rhs_noalloc
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(abi.Params), C.c_void_p, C.c_void_p, C.c_void_p]
+    p = abi.default_params(nx=64, ny=64)
+    # an array starting 8 bytes past a 16-byte boundary
+    assert f(C.byref(p), C.c_void_p(0x10008), C.c_void_p(0x20000), None) == abi.ERR_INVALID
+    assert f(C.byref(p), C.c_void_p(0x10000), C.c_void_p(0x20008), None) == abi.ERR_INVALID
+    # KOLM forcing whose mode lies outside the array
+    q = abi.default_params(nx=64, ny=64, forcing=abi.FORCING_KOLM, force_k=64 * 33, force_scale=1.0)
+    assert f(C.byref(q), C.c_void_p(0x10000), C.c_void_p(0x20000), None) == abi.ERR_INVALID
+    # model and integrator out of range
+    q = abi.default_params(nx=64, ny=64)
+    q.model = 2
+    assert f(C.byref(q), C.c_void_p(0x10000), C.c_void_p(0x20000), None) == abi.ERR_INVALID
+    q = abi.default_params(nx=64, ny=64, integrator=7)
+    assert f(C.byref(q), C.c_void_p(0x10000), C.c_void_p(0x20000), None) == abi.ERR_INVALID

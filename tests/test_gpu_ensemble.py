@@ -1,4 +1,4 @@
-"""Batched ensembles on the GPU (BASELINE config 4 shape, scaled down).
+"""Batched ensembles on the GPU (the uneven 64-member ensemble workload, scaled down).
 
 FP64 members must reproduce single-trajectory handles (same per-column and
 per-row arithmetic; only the launch grouping differs), to 1e-14 of max|w_hat|.

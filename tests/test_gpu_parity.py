@@ -99,7 +99,7 @@ def test_steps_at_grid_size_limits(n, integ):
 
 
 def test_kolmogorov_1024_fp64_steps():
-    """BASELINE config 3 (FP64): Kolmogorov n = 4, F = 1, nu = 1e-4 plus
+    """The 1024^2 Kolmogorov workload (FP64): Kolmogorov n = 4, F = 1, nu = 1e-4 plus
     hyperviscosity nu_h k^16 through the RK4CN drag branch, dt = 2.5e-4."""
     n = 1024
     p = abi.default_params(nx=n, ny=n, nu=1e-4, ekmn_drag_flag=1, ekmn_alpha=2e-40, ekmn_drag_pow=8.0,
@@ -153,7 +153,7 @@ def test_taylor_green_time_convergence(integ, order, quirks, nu, sizes):
 
 
 def test_decaying_256_houli_cfl():
-    """BASELINE config 2 shape: 256^2, nu = 5e-4, Hou-Li filter (reference's
+    """The decaying-turbulence workload shape: 256^2, nu = 5e-4, Hou-Li filter (reference's
     integer form), CFL 0.9 adaptive step; 20 steps with dt from GetTimestep."""
     n = 256
     p = abi.default_params(nx=n, ny=n, nu=5e-4, dealias=abi.DEALIAS_HOU_LI, adapt_step_flag=1,

@@ -23,7 +23,7 @@ def test_oracle_reproduces_reference_fixture(name):
 
 
 def test_taylor_green_decay_matches_analytic():
-    """w0 = 2 sin x sin y, nu = 0.01, dt = 1e-3, 100 steps:
+    """The 64^2 Taylor-Green workload: w0 = 2 sin x sin y, nu = 0.01, dt = 1e-3, 100 steps:
     the amplitude decays as exp(-2 nu t) (solver.c:2526-2530)."""
     p, w0, outs = load_case("tg64_rk4cn")
     w100 = outs[0]

@@ -52,6 +52,62 @@ def test_noalloc_rhs_matches_handle_rhs_twice(n, kw):
     s.close()
 
 
+@pytest.mark.parametrize("n", [16, 32, 64])
+def test_noalloc_rhs_recorded_in_a_captured_graph_houli(n):
+    """The use the entry point exists for: a caller that records the call into
+    its own CUDA graph.  One call outside the capture does the per-device
+    set-up; the call recorded inside torch.cuda.graph is then replayed on new
+    input placed in the captured buffer, and equals the handle's RHS (Hou-Li
+    dealiasing, the small grids with their own tile shapes)."""
+    import torch
+
+    L = load()
+    p = abi.default_params(nx=n, ny=n, nu=1e-3, dealias=abi.DEALIAS_HOU_LI)
+    s = Solver(p)
+    nyf = n // 2 + 1
+    d_in = torch.zeros(2 * n * nyf, dtype=torch.float64, device="cuda")
+    d_out = torch.zeros_like(d_in)
+    assert _noalloc(L, p, d_in.data_ptr(), d_out.data_ptr(), torch.cuda.current_stream().cuda_stream) == abi.OK
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rc = _noalloc(L, p, d_in.data_ptr(), d_out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == abi.OK
+    for seed in (41, 42):
+        w = initial.decaying(n, seed=seed, k0=min(6.0, n / 8), dealias="2/3")
+        expect = s.nonlinear_rhs(w)
+        d_in.copy_(torch.from_numpy(w.view(np.float64).copy()))
+        d_out.fill_(float("nan"))
+        g.replay()
+        torch.cuda.synchronize()
+        got = d_out.cpu().numpy().view(np.complex128).reshape(n, nyf)
+        err = np.max(np.abs(got - expect)) / np.max(np.abs(expect))
+        assert err <= RHS_TOL, (n, seed, err)
+    del g
+    s.close()
+
+
+def test_noalloc_rejects_misaligned_arrays():
+    """A float64 view that starts 8 bytes into an allocation is refused
+    before anything is launched; the context stays usable."""
+    import torch
+
+    L = load()
+    n = 64
+    p = abi.default_params(nx=n, ny=n)
+    elems = 2 * n * (n // 2 + 1)
+    # one spare double each, so that the offset views stay inside their buffers
+    a = torch.zeros(elems + 2, dtype=torch.float64, device="cuda")
+    b = torch.zeros(elems + 2, dtype=torch.float64, device="cuda")
+    assert a.data_ptr() % 16 == 0 and b.data_ptr() % 16 == 0
+    assert _noalloc(L, p, a.data_ptr() + 8, b.data_ptr(), 0) == abi.ERR_INVALID
+    assert _noalloc(L, p, a.data_ptr(), b.data_ptr() + 8, 0) == abi.ERR_INVALID
+    torch.cuda.synchronize()
+    # the same arrays on the 16-byte boundary are taken
+    assert _noalloc(L, p, a.data_ptr(), b.data_ptr(), 0) == abi.OK
+    torch.cuda.synchronize()
+
+
 def test_noalloc_rejects_sizes_above_limit():
     import torch
 
