@@ -404,6 +404,95 @@ ns2d_status dp5_step_impl(ns2d_handle* h, double dt, double* err) {
     return NS2D_OK;
 }
 
+// RK5DPStep (Solver/src/solver.c:360-570) as the reference writes it, with the
+// three defects that stop it compiling fixed (err_sum starts at 0, one surplus
+// parenthesis, w_hat_last read from Int_data): the stages use the table of
+// :35-43 (a32 = 0.5) on the nonlinear term alone, each stage input is the live
+// state plus dt sum a k, every RHS evaluation applies the ForceConjugacy side
+// effect to the state, the update takes Crank-Nicolson factors on the
+// fifth-order sum, and for iters > 1 the error norm is the RMS of the real
+// parts scaled by the state of the previous error step.
+template <typename Real>
+ns2d_status rk5dp_step_impl(ns2d_handle* h, double dt, int iters, double* err) {
+    using C = Cplx<Real>;
+    static const double A[6][6] = {
+        {0.2, 0, 0, 0, 0, 0},
+        {3.0 / 40.0, 0.5, 0, 0, 0, 0},
+        {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+        {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+        {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+        {35.0 / 384.0, 0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+    if (!h->dp[0]) {
+        for (void*& p : h->dp) {
+            CK(h, cudaMalloc(&p, h->field_bytes));
+            CK(h, cudaMemsetAsync(p, 0, h->field_bytes, h->stream));
+        }
+        CK(h, cudaMalloc((void**)&h->dp_kptr, sizeof(void*) * 7));
+        CK(h, cudaMemcpy((void*)h->dp_kptr, h->dp, sizeof(void*) * 7, cudaMemcpyHostToDevice));
+    }
+    if (!h->dp_last) {
+        CK(h, cudaMalloc(&h->dp_last, h->field_bytes));
+        CK(h, cudaMemsetAsync(h->dp_last, 0, h->field_bytes, h->stream));
+    }
+    compute_forcing(h, dt);
+    const bool euler = h->p.system == NS2D_EULER;
+    const int branch = euler ? 4 : resolve_branch(h, false);
+    const bool conj_quirk = quirk(h, NS2D_QUIRK_CONJ_STATE);
+    void* x = h->dp[8];
+    for (int s = 0; s < 7; ++s) {
+        const void* xs = h->state;
+        if (s > 0) {
+            DpCoef cf{};
+            cf.n = s;
+            for (int r = 0; r < s; ++r) cf.c[r] = dt * A[s - 1][r];
+            const C* k[6];
+            for (int r = 0; r < 6; ++r) k[r] = (const C*)h->dp[r];
+            dpw_combine_kernel<Real><<<296, 256, 0, h->stream>>>((C*)x, (const C*)h->state, k[0], k[1], k[2], k[3],
+                                                                k[4], k[5], cf, h->nx, h->nyf, h->ldc);
+            h->launches++;
+            xs = x;
+        }
+        ColArgs<Real> a;
+        fill_common<Real>(h, a, branch);
+        a.src = (const C*)xs;
+        launch_col<Real>(h, COL_P1, a);
+        launch_row<Real>(h);
+        fill_common<Real>(h, a, branch);
+        a.src = (const C*)h->nl;
+        a.rhs_store = (C*)h->dp[s];
+        // NonlinearRHSBatch ends with ForceConjugacy of its input (solver.c:1031)
+        a.conj_mode = (conj_quirk || s == 0) ? 1 : 0;
+        a.conj_src = (const C*)xs;
+        a.conj_stride = h->ldc;
+        a.lin_stage = 0;
+        launch_col<Real>(h, COL_RHS, a);
+    }
+    DpCoef b5{}, bs{};
+    const double B5[7] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
+    const double BS[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0, -92097.0 / 339200.0,
+                          187.0 / 2100.0, 1.0 / 40.0};
+    for (int r = 0; r < 7; ++r) {
+        b5.c[r] = B5[r];
+        bs.c[r] = BS[r];
+    }
+    b5.n = bs.n = 7;
+    dpw_final_kernel<Real><<<296, 256, 0, h->stream>>>((C*)h->state, (C*)h->dp_last, (const C* const*)h->dp_kptr, b5,
+                                                      bs, dt, euler ? 1 : 0, make_lin(h, branch), iters, h->nx,
+                                                      h->nyf, h->ldc, h->dpart);
+    h->launches++;
+    CKL(h);
+    if (iters > 1) {
+        double part[296];
+        CK(h, cudaMemcpyAsync(part, h->dpart, sizeof(part), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        double sum = 0.0;
+        for (int b = 0; b < 296; ++b) sum += part[b];
+        h->dp_err = std::sqrt(1.0 / (double)((long)h->nx * (long)h->nyf) * sum);
+    }
+    *err = h->dp_err;
+    return NS2D_OK;
+}
+
 // c2r of up to two spectral fields to x-space (f[0], f[1]) followed by a row
 // pass with a reduction or a store.
 template <typename Real>
@@ -506,7 +595,7 @@ void fill_twiddles(std::vector<Cplx<Real>>& tw, int n) {
 void free_all(ns2d_handle* h) {
     void* ptrs[] = {h->state, h->acc, h->nl, h->f[0], h->f[1], h->f[2], h->f[3], h->tmpfull, h->col0[0], h->col0[1],
                     h->tw, h->rhsbuf, h->ab[0], h->ab[1], h->ab[2], h->ab[3], h->uhat_ref, h->dreal, h->dscal, h->dmax,
-                    h->dstatus, h->dio, h->ddiag, h->dpart, h->cn};
+                    h->dstatus, h->dio, h->ddiag, h->dpart, h->cn, h->dp_last};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : h->dp)
@@ -1317,6 +1406,15 @@ ns2d_status ns2d_dp5_step(ns2d_handle* h, double dt, double* err) {
     cudaSetDevice(h->p.device);
     if (h->p.model != NS2D_MODEL_FULL) return fail(h, NS2D_ERR_UNSUPPORTED, "the DP5 step has no phase-only form");
     ns2d_status s = DISPATCH(h, dp5_step_impl, h, dt, err);
+    if (s) return s;
+    return check_status(h);
+}
+
+ns2d_status ns2d_rk5dp_step(ns2d_handle* h, double dt, int32_t iters, double* err) {
+    if (!h || !err || !(dt > 0.0) || iters < 1) return NS2D_ERR_INVALID;
+    cudaSetDevice(h->p.device);
+    if (h->p.model != NS2D_MODEL_FULL) return fail(h, NS2D_ERR_UNSUPPORTED, "RK5DPStep's phase-only reset does not compile");
+    ns2d_status s = DISPATCH(h, rk5dp_step_impl, h, dt, (int)iters, err);
     if (s) return s;
     return check_status(h);
 }

@@ -427,4 +427,120 @@ __global__ void __launch_bounds__(256) dp_final_kernel(typename Cx<Real>::T* __r
     }
 }
 
+// RK5DPStep as the reference writes it (Solver/src/solver.c:404-466): stage
+// input X = w + (dt a_1) k_1 + (dt a_2) k_2 + ..., summed left to right from
+// the live state w, skipping the zero coefficients the reference leaves out
+// (the a72 of the seventh stage).  cf.c[r] holds the products dt * a_r.
+template <typename Real>
+__global__ void dpw_combine_kernel(typename Cx<Real>::T* __restrict__ x, const typename Cx<Real>::T* __restrict__ w,
+                                   const typename Cx<Real>::T* k0, const typename Cx<Real>::T* k1,
+                                   const typename Cx<Real>::T* k2, const typename Cx<Real>::T* k3,
+                                   const typename Cx<Real>::T* k4, const typename Cx<Real>::T* k5, DpCoef cf,
+                                   int nx, int nyf, int ldc) {
+    using C = typename Cx<Real>::T;
+    const C* ks[6] = {k0, k1, k2, k3, k4, k5};
+    const long long n = (long long)nx * nyf;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const size_t o = (size_t)(q / nyf) * ldc + (size_t)(q % nyf);
+        const C y = w[o];
+        double xr = (double)y.x, xi = (double)y.y;
+        for (int r = 0; r < cf.n; ++r) {
+            if (cf.c[r] == 0.0) continue;
+            const C v = ks[r][o];
+            xr = xr + cf.c[r] * (double)v.x;
+            xi = xi + cf.c[r] * (double)v.y;
+        }
+        x[o] = cmake<C>((Real)xr, (Real)xi);
+    }
+}
+
+// Update and error of RK5DPStep as written (Solver/src/solver.c:470-566):
+//   w <- w (2 - D)/(2 + D) + 2 dt/(2 + D) (b1 k1 + b3 k3 + b4 k4 + b5 k5 + b6 k6)
+// (explicit w + sum dt (b k) for the Euler system), the mean mode 0; then, when
+// iters > 1, the error sum of the real parts (dp_ho_step is a double and pow()
+// takes the real part of its complex argument):
+//   ho = Re(w_new + (sum_{s<=6} dt (bs_s k_s)) + dt (bs7 k7)),
+//   e  = (Re w_new - ho) / (DP_ABS_TOL + max(|w_last|, |w_new|) DP_REL_TOL),
+// one FP64 partial of sum e^2 per block, and w_last <- w_new.
+template <typename Real>
+__global__ void __launch_bounds__(256) dpw_final_kernel(typename Cx<Real>::T* __restrict__ state,
+                                                        typename Cx<Real>::T* __restrict__ w_last,
+                                                        const typename Cx<Real>::T* const* __restrict__ k, DpCoef b5,
+                                                        DpCoef bs, double dt, int euler, LinOp lin, int iters, int nx,
+                                                        int nyf, int ldc, double* partials) {
+    using C = typename Cx<Real>::T;
+    const long long n = (long long)nx * nyf;
+    double acc = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / nyf), j = (int)(q % nyf);
+        const size_t o = (size_t)i * ldc + j;
+        if (i == 0 && j == 0) {
+            state[o] = cmake<C>(0, 0);
+            if (iters > 1) w_last[o] = cmake<C>(0, 0);
+            continue;
+        }
+        const int kx = (i <= nx / 2) ? i : i - nx;
+        const C w = state[o];
+        double wr, wi;
+        if (euler) {
+            double sr = 0.0, si = 0.0;
+            bool first = true;
+            for (int r = 0; r < 7; ++r) {
+                if (b5.c[r] == 0.0) continue;
+                const C v = k[r][o];
+                const double tr = dt * (b5.c[r] * (double)v.x), ti = dt * (b5.c[r] * (double)v.y);
+                sr = first ? tr : sr + tr;
+                si = first ? ti : si + ti;
+                first = false;
+            }
+            wr = (double)w.x + sr;
+            wi = (double)w.y + si;
+        } else {
+            double sr = 0.0, si = 0.0;
+            bool first = true;
+            for (int r = 0; r < 7; ++r) {
+                if (b5.c[r] == 0.0) continue;
+                const C v = k[r][o];
+                const double tr = b5.c[r] * (double)v.x, ti = b5.c[r] * (double)v.y;
+                sr = first ? tr : sr + tr;
+                si = first ? ti : si + ti;
+                first = false;
+            }
+            const double D = dt * lin_bracket(lin, (double)(kx * kx + j * j));
+            const double f1 = (2.0 - D) / (2.0 + D), f2 = (2.0 * dt) / (2.0 + D);
+            wr = (double)w.x * f1 + f2 * sr;
+            wi = (double)w.y * f1 + f2 * si;
+        }
+        const C wn = cmake<C>((Real)wr, (Real)wi);
+        if (iters > 1) {
+            double hr = 0.0;
+            bool first = true;
+            for (int r = 0; r < 6; ++r) {
+                if (bs.c[r] == 0.0) continue;
+                const double t = dt * (bs.c[r] * (double)k[r][o].x);
+                hr = first ? t : hr + t;
+                first = false;
+            }
+            const double ho = ((double)wn.x + hr) + dt * (bs.c[6] * (double)k[6][o].x);
+            const C wl = w_last[o];
+            const double a = hypot((double)wl.x, (double)wl.y), b = hypot((double)wn.x, (double)wn.y);
+            const double denom = 1e-7 + (a > b ? a : b) * 1e-7;
+            const double e = ((double)wn.x - ho) / denom;
+            acc += e * e;
+            w_last[o] = wn;
+        }
+        state[o] = wn;
+    }
+    __shared__ double red[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        partials[blockIdx.x] = tot;
+    }
+}
+
 }  // namespace ns2d

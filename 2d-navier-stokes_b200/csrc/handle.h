@@ -72,6 +72,10 @@ struct ns2d_handle {
     // Dormand-Prince stages k0..k6, y0 and the stage input (allocated on first use)
     void* dp[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     const void** dp_kptr = nullptr;  // device array of the seven stage pointers
+    // RK5DPStep as written: the state of the last error step (Int_data->w_hat_last,
+    // zero until then) and the last error (Int_data->DP_err)
+    void* dp_last = nullptr;
+    double dp_err = 0.0;
     // one RK4/RK4CN step captured as a CUDA graph for fixed-dt stepping
     cudaGraphExec_t step_graph = nullptr;
     int graph_kernels = 9;  // kernels in one captured step

@@ -66,6 +66,7 @@ def load():
         "ns2d_set_kernel_timing": (C.c_int, [H, C.c_int32]),
         "ns2d_kernel_times": (C.c_int, [H, _dp, C.POINTER(C.c_int64), C.c_int32]),
         "ns2d_dp5_step": (C.c_int, [H, C.c_double, _dp]),
+        "ns2d_rk5dp_step": (C.c_int, [H, C.c_double, C.c_int32, _dp]),
         "ns2d_set_forcing_modes": (C.c_int, [H, C.c_int32, C.POINTER(C.c_int32), _dp]),
         "ns2d_adjoint_record": (C.c_int, [H, C.c_int32, C.c_double, C.c_int32]),
         "ns2d_adjoint_backward": (C.c_int, [H, _dp, _dp]),

@@ -133,6 +133,13 @@ class Solver:
         self._ck(self.L.ns2d_dp5_step(self.h, dt, C.byref(e)))
         return e.value
 
+    def rk5dp_step(self, dt, iters):
+        """RK5DPStep as the reference writes it, at SpectralSolve iteration
+        `iters`; returns DP_err (unchanged when iters == 1)."""
+        e = C.c_double()
+        self._ck(self.L.ns2d_rk5dp_step(self.h, dt, int(iters), C.byref(e)))
+        return e.value
+
     def step_n(self, n, dt):
         self._ck(self.L.ns2d_step_n(self.h, n, dt))
 

@@ -185,6 +185,22 @@ ns2d_status ns2d_ab4_step(ns2d_handle* h, double dt, int32_t iters);
    retrying is the caller's (dt_new = dt min(1.5, max(0.01, 0.8 err^-1/5))). */
 ns2d_status ns2d_dp5_step(ns2d_handle* h, double dt, double* err);
 
+/* RK5DPStep (Solver/src/solver.c:360-570; solver.h:33) as the reference writes
+   it, for parity with the reference's own arithmetic; ns2d_dp5_step is the
+   corrected integrator.  The reference's three compile defects are fixed
+   (err_sum starts at 0, a surplus parenthesis at :517, w_hat_last read from
+   Int_data at :564); everything else is kept: the Butcher table of :35-43
+   (its a32 is 0.5, not 9/40) on the nonlinear term alone, stage inputs built
+   from the live state (which every RHS rewrites through the ForceConjugacy
+   side effect), the Crank-Nicolson update of the fifth-order sum, and, for
+   iters > 1 only, the error norm of :515-552: RMS over the half spectrum of
+   Re(w_new - ho) / (1e-7 + 1e-7 max(|w_last|, |w_new|)) with ho the real part
+   of w_new + dt sum bs k (the reference stores it in a double) and w_last
+   the state after the previous error step (0 before it).  iters is
+   SpectralSolve's iteration counter; *err = DP_err, unchanged when iters == 1
+   (0 on a fresh handle).  The state is advanced. */
+ns2d_status ns2d_rk5dp_step(ns2d_handle* h, double dt, int32_t iters, double* err);
+
 /* nsteps fixed-dt steps of the configured integrator without host round trips
    (the loop body of SpectralSolve, solver.c:142-236, minus saving). */
 ns2d_status ns2d_step_n(ns2d_handle* h, int32_t nsteps, double dt);

@@ -62,6 +62,8 @@ struct ns2d_oracle {
     double w_max_init;
     double min_dt, max_dt;
     int n_spect;
+    cplx* w_hat_last; /* Int_data->w_hat_last (RK5DPStep as written)   */
+    double dp_err;    /* Int_data->DP_err                              */
 };
 
 static int quirk(const ns2d_oracle* o, int bit) { return (o->p.quirks & bit) != 0; }
@@ -89,6 +91,7 @@ ns2d_oracle* oracle_create(const ns2d_params* p, int threads) {
     o->rk_tmp = (cplx*)calloc(o->ns, sizeof(cplx));
     for (int s = 0; s < 3; ++s) o->ab_hist[s] = (cplx*)calloc(o->ns, sizeof(cplx));
     o->ab_tmp = (cplx*)calloc(o->ns, sizeof(cplx));
+    o->w_hat_last = (cplx*)calloc(o->ns, sizeof(cplx));
     o->u_hat2 = (cplx*)calloc(2 * o->ns, sizeof(cplx));
     o->pair = (cplx*)calloc(2 * o->ns, sizeof(cplx));
     size_t nr = (size_t)o->nx * (o->ny + 2);
@@ -115,7 +118,7 @@ void oracle_destroy(ns2d_oracle* o) {
     for (int s = 0; s < 7; ++s) free(o->rk[s]);
     free(o->rk_tmp);
     for (int s = 0; s < 3; ++s) free(o->ab_hist[s]);
-    free(o->ab_tmp); free(o->u_hat2); free(o->pair);
+    free(o->ab_tmp); free(o->w_hat_last); free(o->u_hat2); free(o->pair);
     free(o->real2a); free(o->real2b); free(o->real1);
     free(o);
 }
@@ -433,6 +436,87 @@ int oracle_dp5_step(ns2d_oracle* o, double dt, double* err) {
     *err = sqrt(sum / (double)(o->nx * o->nyf));
     free(y0);
     return 0;
+}
+
+/* RK5DPStep as the reference writes it (Solver/src/solver.c:360-570), with
+   the three defects that stop it compiling fixed the way oracle/Makefile's
+   dp5 build fixes them (err_sum starts at 0, one surplus parenthesis, the
+   w_hat_last member read from Int_data).  Everything else is kept:
+   * the table of :35-43, whose a32 is 0.5 (the published Dormand-Prince value
+     is 9/40), on the nonlinear term alone; each stage input is the live state
+     plus dt sum a k, and every NonlinearRHSBatch call rewrites the state's
+     ky = 0, kx < 0 modes from its input (the ForceConjugacy side effect);
+   * the update of :494-514: Crank-Nicolson factors on the fifth-order sum
+     (explicit for the Euler system);
+   * the error of :515-552, only when iters > 1: dp_ho_step is a double, so it
+     keeps the real part of w_new + dt sum bs k, pow() keeps the real part of
+     its complex argument, the scale uses the state of the previous error step
+     (w_hat_last, 0 until the first one), and DP_err = sqrt(sum / (Nx Nyf)).
+   Returns DP_err, which keeps its previous value when iters == 1. */
+static const double kR5_A32 = 0.5;
+double oracle_rk5dp_step(ns2d_oracle* o, double dt, int iters) {
+    cplx** k = o->rk;
+    cplx* w = o->w_hat;
+    cplx* x = o->rk_tmp;
+    const size_t ns = o->ns;
+    oracle_compute_forcing(o, dt);
+    nonlinear_rhs(o, w, k[0]);
+    for (size_t idx = 0; idx < ns; ++idx) x[idx] = w[idx] + dt * kDP_A21 * k[0][idx];
+    nonlinear_rhs(o, x, k[1]);
+    for (size_t idx = 0; idx < ns; ++idx)
+        x[idx] = w[idx] + dt * kDP_A31 * k[0][idx] + dt * kR5_A32 * k[1][idx];
+    nonlinear_rhs(o, x, k[2]);
+    for (size_t idx = 0; idx < ns; ++idx)
+        x[idx] = w[idx] + dt * kDP_A41 * k[0][idx] + dt * kDP_A42 * k[1][idx] + dt * kDP_A43 * k[2][idx];
+    nonlinear_rhs(o, x, k[3]);
+    for (size_t idx = 0; idx < ns; ++idx)
+        x[idx] = w[idx] + dt * kDP_A51 * k[0][idx] + dt * kDP_A52 * k[1][idx] + dt * kDP_A53 * k[2][idx] +
+                 dt * kDP_A54 * k[3][idx];
+    nonlinear_rhs(o, x, k[4]);
+    for (size_t idx = 0; idx < ns; ++idx)
+        x[idx] = w[idx] + dt * kDP_A61 * k[0][idx] + dt * kDP_A62 * k[1][idx] + dt * kDP_A63 * k[2][idx] +
+                 dt * kDP_A64 * k[3][idx] + dt * kDP_A65 * k[4][idx];
+    nonlinear_rhs(o, x, k[5]);
+    /* stage 7 input: the a7 row equals the fifth-order weights b */
+    for (size_t idx = 0; idx < ns; ++idx)
+        x[idx] = w[idx] + dt * kDP_B1 * k[0][idx] + dt * kDP_B3 * k[2][idx] + dt * kDP_B4 * k[3][idx] +
+                 dt * kDP_B5 * k[4][idx] + dt * kDP_B6 * k[5][idx];
+    nonlinear_rhs(o, x, k[6]);
+    double err_sum = 0.0;
+    for (int i = 0; i < o->nx; ++i)
+        for (int j = 0; j < o->nyf; ++j) {
+            size_t idx = (size_t)i * o->nyf + j;
+            if (o->kx[i] != 0 || o->ky[j] != 0) {
+                if (o->p.system == NS2D_EULER) {
+                    w[idx] = w[idx] + (dt * (kDP_B1 * k[0][idx]) + dt * (kDP_B3 * k[2][idx]) +
+                                       dt * (kDP_B4 * k[3][idx]) + dt * (kDP_B5 * k[4][idx]) +
+                                       dt * (kDP_B6 * k[5][idx]));
+                } else {
+                    double k_sqr = (double)(o->kx[i] * o->kx[i] + o->ky[j] * o->ky[j]);
+                    double D = dt * lin_bracket(o, k_sqr, 0);
+                    w[idx] = w[idx] * ((2.0 - D) / (2.0 + D)) +
+                             (2.0 * dt / (2.0 + D)) * (kDP_B1 * k[0][idx] + kDP_B3 * k[2][idx] + kDP_B4 * k[3][idx] +
+                                                       kDP_B5 * k[4][idx] + kDP_B6 * k[5][idx]);
+                }
+                if (iters > 1) {
+                    double ho = creal(w[idx] + (dt * (kDP_E1 * k[0][idx]) + dt * (kDP_E3 * k[2][idx]) +
+                                                dt * (kDP_E4 * k[3][idx]) + dt * (kDP_E5 * k[4][idx]) +
+                                                dt * (kDP_E6 * k[5][idx])) +
+                                      dt * (kDP_E7 * k[6][idx]));
+                    double a = cabs(o->w_hat_last[idx]), b = cabs(w[idx]);
+                    double denom = 1e-7 + (a > b ? a : b) * 1e-7;
+                    err_sum += pow(creal((w[idx] - ho) / denom), 2.0);
+                }
+            } else {
+                w[idx] = 0.0;
+            }
+        }
+    if (iters > 1) {
+        o->dp_err = sqrt(1.0 / (double)((long)o->nx * (long)o->nyf) * err_sum);
+        for (size_t idx = 0; idx < ns; ++idx) o->w_hat_last[idx] = w[idx];
+        o->w_hat_last[0] = 0.0;
+    }
+    return o->dp_err;
 }
 
 /* c2r of the state, normalised by 1/(NxNy) (Solver/src/solver.c:2218-2230). */

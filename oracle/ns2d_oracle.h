@@ -30,6 +30,7 @@ void oracle_nonlinear_rhs(ns2d_oracle* o, const double* in, double* out);
 void oracle_rk4_step(ns2d_oracle* o, double dt);
 int oracle_ab4_step(ns2d_oracle* o, double dt, int iters);
 int oracle_dp5_step(ns2d_oracle* o, double dt, double* err);
+double oracle_rk5dp_step(ns2d_oracle* o, double dt, int iters);
 void oracle_apply_dealiasing(const ns2d_oracle* o, double* arr, int array_dim);
 void oracle_force_conjugacy(ns2d_oracle* o, const double* arr);
 double oracle_get_max_data(ns2d_oracle* o, int kind);

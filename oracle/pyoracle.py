@@ -62,6 +62,8 @@ class Oracle:
             L.oracle_rk4_step.argtypes = [C.c_void_p, C.c_double]
             L.oracle_ab4_step.argtypes = [C.c_void_p, C.c_double, C.c_int]
             L.oracle_dp5_step.argtypes = [C.c_void_p, C.c_double, _dp]
+            L.oracle_rk5dp_step.argtypes = [C.c_void_p, C.c_double, C.c_int]
+            L.oracle_rk5dp_step.restype = C.c_double
             L.oracle_apply_dealiasing.argtypes = [C.c_void_p, _dp, C.c_int]
             L.oracle_get_max_data.argtypes = [C.c_void_p, C.c_int]
             L.oracle_get_max_data.restype = C.c_double
@@ -130,6 +132,10 @@ class Oracle:
         self.L.oracle_dp5_step(self.h, dt, _ptr(e))
         return float(e[0])
 
+    def rk5dp_step(self, dt, iters):
+        """RK5DPStep as the reference writes it, at iteration `iters`; DP_err."""
+        return self.L.oracle_rk5dp_step(self.h, dt, iters)
+
     def apply_dealiasing(self, arr, dim=1):
         a = np.ascontiguousarray(arr, np.complex128).copy()
         self.L.oracle_apply_dealiasing(self.h, _ptr(a.view(np.float64)), dim)
@@ -197,7 +203,11 @@ class RefSolver:
         for f in ("ref_set_w_hat", "ref_get_w_hat", "ref_nonlinear_rhs_state", "ref_get_w_real"):
             getattr(L, f).argtypes = [_dp]
         L.ref_nonlinear_rhs_input.argtypes = [_dp, _dp]
-        L.ref_rk4_step.argtypes = [C.c_double]
+        if hasattr(L, "ref_rk4_step"):  # absent from the Dormand-Prince build
+            L.ref_rk4_step.argtypes = [C.c_double]
+        if variant == "dp5":
+            L.ref_dp5_step.argtypes = [C.c_double, C.c_int]
+            L.ref_dp5_step.restype = C.c_double
         if variant == "ab4":
             L.ref_ab4_step.argtypes = [C.c_double, C.c_int]
         L.ref_compute_forcing.argtypes = [C.c_double]
@@ -253,6 +263,10 @@ class RefSolver:
 
     def ab4_step(self, dt, iters):
         self.L.ref_ab4_step(dt, iters)
+
+    def rk5dp_step(self, dt, iters):
+        """RK5DPStep at iteration `iters` (variant "dp5"); returns DP_err."""
+        return self.L.ref_dp5_step(dt, iters)
 
     def apply_dealiasing(self, arr, dim=1):
         a = np.ascontiguousarray(arr, np.complex128).copy()

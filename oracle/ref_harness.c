@@ -58,7 +58,9 @@ typedef struct ref_params {
 } ref_params;
 
 int ref_variant(void) {
-#if defined(__AB4)
+#if defined(__DPRK5)
+    return 3;
+#elif defined(__AB4)
     return 2;
 #elif defined(__RK4)
     return 1;
@@ -109,6 +111,17 @@ int ref_init(const ref_params* p, int run_initial_conditions, int threads) {
     if (g_ready) return -1;
     set_globals(p, threads);
     const long int NBatch[2] = {p->nx, p->ny / 2 + 1};
+#if defined(__DPRK5)
+    /* AllocateMemory's __DPRK5 branch zeroes the Adams-Bashforth arrays
+       (Solver/src/solver.c:2850-2856), which only its __AB4 branch allocates
+       (:2774-2791); the harness provides them so that the reference's own
+       AllocateMemory runs unchanged.  They live for the process. */
+    {
+        const size_t batch = 2 * (size_t)p->nx * (size_t)(p->ny / 2 + 1);
+        g_int.AB_tmp = (fftw_complex*)calloc(batch, sizeof(fftw_complex));
+        for (int a = 0; a < 3; ++a) g_int.AB_tmp_nonlin[a] = (fftw_complex*)calloc(batch, sizeof(fftw_complex));
+    }
+#endif
     AllocateMemory(NBatch, &g_int);
     InitializeFFTWPlans(g_N);
     InitializeSpaceVariables(run_data->x, run_data->k, g_N);
@@ -133,7 +146,19 @@ int ref_hyper_visc_flag(void) { return sys_vars->HYPER_VISC_FLAG; }
 void ref_set_hyper_visc_flag(int f) { sys_vars->HYPER_VISC_FLAG = f; }
 void ref_compute_forcing(double dt) { ComputeForcing(dt); }
 
+#if defined(__RK4) || defined(__RK4CN) || defined(__AB4)
 void ref_rk4_step(double dt) { RK4Step(dt, g_N, sys_vars->local_Nx, &g_int); }
+#endif
+
+#if defined(__DPRK5)
+/* One RK5DPStep (Solver/src/solver.c:360-570) at SpectralSolve iteration
+   `iters`, called directly (SpectralSolve's accept/retry loop, :150-171, is
+   not run); returns Int_data->DP_err, which the step sets only when iters > 1. */
+double ref_dp5_step(double dt, int iters) {
+    RK5DPStep(dt, g_N, iters, sys_vars->local_Nx, &g_int);
+    return g_int.DP_err;
+}
+#endif
 
 #if defined(__AB4)
 void ref_ab4_step(double dt, int iters) { AB4Step(dt, g_N, iters, sys_vars->local_Nx, &g_int); }

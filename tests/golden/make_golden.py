@@ -68,6 +68,16 @@ def cases():
         "po32_houli": ("houli_po", dict(nx=32, ny=32, nu=5e-4, dealias=abi.DEALIAS_HOU_LI,
                                         model=abi.MODEL_PHASE_ONLY, dt=1e-3),
                        ("decaying", 14, 6.0, None, "houli_ic"), [("po_steps", 10, 1e-3), ("w_hat",)]),
+        # RK5DPStep as written (reference built with -D__DPRK5 from a copy with
+        # its three compile defects fixed, oracle/Makefile): DP_err of
+        # SpectralSolve iterations 1..6 (0 at the first, which computes none),
+        # then the state; stock flags (the hyperviscosity bracket with == only)
+        "dp5_32": ("dp5", dict(nx=32, ny=32, nu=1e-3, dt=1e-3),
+                   ("decaying", 16, 4.0), [("rk5dp", 6, 1e-3), ("w_hat",)]),
+        # the same with drag + hyperviscosity on alpha |k|^16 and Kolmogorov forcing
+        "dp5_32_kolm": ("dp5", dict(nx=32, ny=32, nu=1e-3, ekmn_drag_flag=1, ekmn_alpha=1e-12, ekmn_drag_pow=8.0,
+                                    forcing=abi.FORCING_KOLM, force_k=4, force_scale=1.0, dt=2e-3),
+                        ("decaying", 17, 4.0), [("rk5dp", 6, 2e-3), ("w_hat",), ("meas",)]),
         # adaptive CFL step with the reference's row-index quirk
         "cfl32": ("rk4cn", dict(nx=32, ny=32, nu=1e-3, adapt_step_flag=1, cfl_cond_flag=1, cfl_const=0.9, dt=1e-3),
                   ("decaying", 6, 4.0), [("cfl", 1e-3), ("steps", 5, 2e-3), ("cfl", 2e-3), ("w_hat",)]),
@@ -117,6 +127,8 @@ def run_program(solver, w0, program, record):
         elif kind == "ab4":
             for it in range(1, op[1] + 1):
                 solver.ab4_step(op[2], it)
+        elif kind == "rk5dp":
+            outs.append(np.array([solver.rk5dp_step(op[2], it) for it in range(1, op[1] + 1)]))
         elif kind == "w_hat":
             outs.append(solver.get_w_hat())
         elif kind == "max":

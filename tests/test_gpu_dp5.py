@@ -1,6 +1,14 @@
-"""Dormand-Prince 5(4) step on the GPU against the oracle's corrected
-restatement of RK5DPStep (Solver/src/solver.c:360-570; the shipped routine does
-not compile, so parity is with the restatement, which is unpinned)."""
+"""Dormand-Prince steps on the GPU.
+
+* ns2d_rk5dp_step is RK5DPStep (Solver/src/solver.c:360-570) as the reference
+  writes it.  Its parity with the reference's own arithmetic is pinned by the
+  golden fixtures dp5_32 and dp5_32_kolm (tests/test_gpu_parity.py), made by the
+  reference built with -D__DPRK5 from a copy with its three compile defects
+  fixed (oracle/Makefile); here it is checked against the oracle's restatement
+  of that build (itself equal to the fixtures to the last bit) on larger grids
+  and with the Hou-Li filter.
+* ns2d_dp5_step is the corrected Dormand-Prince 5(4) integrator, checked
+  against the oracle's corrected restatement."""
 import numpy as np
 import pytest
 
@@ -9,6 +17,27 @@ from ns2d import Solver, abi, initial
 from pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,kw", [
+    (128, dict(nu=1e-3)),
+    (128, dict(nu=1e-3, ekmn_drag_flag=1, ekmn_alpha=1e-20, ekmn_drag_pow=8.0, forcing=abi.FORCING_KOLM, force_k=4,
+               force_scale=1.0)),
+    (64, dict(nu=1e-4, dealias=abi.DEALIAS_HOU_LI, quirks=abi.QUIRKS_REFERENCE)),
+    (512, dict(nu=5e-4)),
+])
+def test_rk5dp_as_written_matches_restatement(n, kw):
+    p = abi.default_params(nx=n, ny=n, **kw)
+    w0 = initial.decaying(n, 5, k0=4.0, dealias="2/3")
+    s, o = Solver(p), Oracle(p, threads=8)
+    s.set_w_hat(w0)
+    o.set_w_hat(w0)
+    for it, dt in enumerate((1e-3, 1e-3, 2e-3, 5e-4, 5e-4), start=1):
+        e_gpu = s.rk5dp_step(dt, it)
+        e_ref = o.rk5dp_step(dt, it)
+        assert abs(e_gpu - e_ref) <= 1e-10 * abs(e_ref), (it, e_gpu, e_ref)
+        assert rel_err(s.get_w_hat(), o.get_w_hat()) <= 1e-12, it
+    assert e_ref > 0.0
 
 
 @pytest.mark.parametrize("n,kw", [
