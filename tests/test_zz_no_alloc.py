@@ -76,7 +76,7 @@ def test_noalloc_rhs_recorded_in_a_captured_graph_houli(n):
     for seed in (41, 42):
         w = initial.decaying(n, seed=seed, k0=min(6.0, n / 8), dealias="2/3")
         expect = s.nonlinear_rhs(w)
-        d_in.copy_(torch.from_numpy(w.view(np.float64).copy()))
+        d_in.copy_(torch.from_numpy(w.view(np.float64).reshape(-1).copy()))
         d_out.fill_(float("nan"))
         g.replay()
         torch.cuda.synchronize()
