@@ -212,6 +212,75 @@ def cpu_reference(steps, warmup, threads, budget_s=None):
     return steps / el, steps, el
 
 
+# The reference's CPU solver on the three FP64 workloads (host cores): the
+# 64^2 Taylor-Green case (nu |k|^2 through the drag flag, dt = 1e-3), the 256^2
+# decaying case (Hou-Li build, CFL 0.9 adaptive step, nu = 5e-4) and the 1024^2
+# Kolmogorov case of the headline metric.
+CPU_TABLE = (("taylor_green_64_fp64_rk4cn", 64), ("decaying_256_houli_cfl_fp64_rk4cn", 256),
+             ("kolmogorov_1024_fp64_rk4cn", 1024))
+
+
+def _cpu_case(name):
+    from ns2d import abi, initial
+    if name.startswith("taylor_green"):
+        p = abi.default_params(nx=64, ny=64, nu=0.01, ekmn_drag_flag=1, ekmn_alpha=0.0, dt=1e-3)
+        return p, "rk4cn", initial.taylor_green(64), False
+    if name.startswith("decaying"):
+        p = abi.default_params(nx=256, ny=256, nu=5e-4, dealias=abi.DEALIAS_HOU_LI, adapt_step_flag=1,
+                               cfl_cond_flag=1, cfl_const=0.9, dt=1e-3)
+        return p, "houli", initial.decaying(256, seed=2, k0=6.0), True
+    return params(), "rk4cn", initial.noise(N, seed=7, amplitude=1e-3, kolm=True), False
+
+
+def _cpu_table_worker(name, thread_counts, runs, budget_s, q):
+    """Median steps/s of `runs` timed runs after one warm-up step, for each
+    thread count, in a process of its own (the reference keeps global state)."""
+    from pyoracle import RefSolver
+    p, variant, w0, adaptive = _cpu_case(name)
+    ref = RefSolver(p, variant, threads=thread_counts[0])
+    ref.set_w_hat(w0)
+    dt = ref.get_timestep(p.dt) if adaptive else p.dt
+    out = []
+    for th in thread_counts:
+        ref.set_threads(th)
+        t0 = time.perf_counter()
+        ref.rk4_step(dt)
+        if adaptive:
+            dt = ref.get_timestep(dt)
+        one = time.perf_counter() - t0
+        k = max(1, min(200, int(budget_s / (runs * max(one, 1e-4)))))
+        rates = []
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            for _ in range(k):
+                ref.rk4_step(dt)
+                if adaptive:
+                    dt = ref.get_timestep(dt)
+            rates.append(k / (time.perf_counter() - t0))
+        out.append({"threads": th, "steps_per_run": k, "runs": runs,
+                    "steps_per_s_median": statistics.median(rates), "steps_per_s_runs": rates})
+    q.put(out)
+
+
+def cpu_table(threads, runs=5, budget_s=4.0):
+    """The reference on each workload at T = threads and T = 1; each case in a
+    spawned process, about budget_s seconds of timed work per thread count."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    rows = []
+    for name, n in CPU_TABLE:
+        q = ctx.Queue()
+        proc = ctx.Process(target=_cpu_table_worker, args=(name, (threads, 1) if threads > 1 else (1,), runs,
+                                                          budget_s, q))
+        proc.start()
+        res = q.get(timeout=600)
+        proc.join(60)
+        for r in res:
+            r.update({"workload": name, "grid": f"{n}x{n}"})
+            rows.append(r)
+    return rows
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -270,6 +339,29 @@ def ensemble_bench(stream, flush, steps, warmup, rank):
     return steps / (ms * 1e-3), ms / steps, grids, launches, z
 
 
+def ensemble_error(stream, steps, rank):
+    """Largest relative enstrophy difference over the 64 members between the
+    FP32 ensemble (tuned grids, graph-replayed steps) and the FP64 ensemble
+    after `steps` steps of the same workload."""
+    from ns2d import Ensemble, abi, initial
+    rng = np.random.default_rng(100 + rank)
+    ics = [initial.decaying(n, seed=1000 * rank + m, k0=float(rng.choice([4, 6, 8])), dealias="2/3")
+           for m, n in enumerate(ENS_SIZES)]
+    z = {}
+    for prec in (abi.FP64, abi.FP32):
+        e = Ensemble(abi.default_params(nu=1e-3, dt=ENS_DT, precision=prec), ENS_SIZES)
+        e.set_stream(stream.cuda_stream)
+        if prec == abi.FP32:
+            e.tune(ENS_DT)
+        for m, w in enumerate(ics):
+            e.set_w_hat(m, w)
+        e.step_n(steps, ENS_DT)
+        z[prec] = np.array([e.measurables(m).enstrophy for m in range(len(ENS_SIZES))])
+        e.close()
+    rel = np.abs(z[abi.FP32] - z[abi.FP64]) / np.abs(z[abi.FP64])
+    return float(rel.max()), int(rel.argmax())
+
+
 ADJ_N, ADJ_DT, ADJ_EVERY = 512, 5e-4, 50
 
 
@@ -321,23 +413,33 @@ def adjoint_bench(stream, nsteps, rank, precision, g_ref=None, n_dirs=16):
            "J_final_enstrophy": J}
     if precision == abi.FP64:
         rng = np.random.default_rng(900 + rank)
-        rel, scaled = [], []
+        eps_list = (1e-5, 1e-6, 1e-7)
+        rel = {e: [] for e in eps_list}
+        scaled = {e: [] for e in eps_list}
         gn = np.sqrt(wdot(g, g))
         for _ in range(n_dirs):
             d = initial.dealias_23(initial.hermitian(rng.standard_normal(w0.shape) + 1j * rng.standard_normal(w0.shape)))
             d *= np.sqrt(wdot(w0, w0) / wdot(d, d))
-            vals = []
-            for sgn in (1.0, -1.0):
-                s.set_w_hat(w0 + sgn * 1e-6 * d)
-                s.step_n(nsteps, ADJ_DT)
-                vals.append(s.objective(abi.OBJ_ENSTROPHY))
-            fd = (vals[0] - vals[1]) / 2e-6
             ad = wdot(g, d)
-            rel.append(abs(fd - ad) / abs(fd))
-            scaled.append(abs(fd - ad) / (gn * np.sqrt(wdot(d, d))))
+            for eps in eps_list:
+                vals = []
+                for sgn in (1.0, -1.0):
+                    s.set_w_hat(w0 + sgn * eps * d)
+                    s.step_n(nsteps, ADJ_DT)
+                    vals.append(s.objective(abi.OBJ_ENSTROPHY))
+                fd = (vals[0] - vals[1]) / (2.0 * eps)
+                rel[eps].append(abs(fd - ad) / abs(fd))
+                scaled[eps].append(abs(fd - ad) / (gn * np.sqrt(wdot(d, d))))
         if n_dirs:
-            out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel),
-                         "median_rel_err": float(np.median(rel)), "max_err_over_grad_norm": max(scaled)}
+            best_rel = [min(rel[e][i] for e in eps_list) for i in range(n_dirs)]
+            best_scaled = [min(scaled[e][i] for e in eps_list) for i in range(n_dirs)]
+            out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel[1e-6]),
+                         "median_rel_err": float(np.median(rel[1e-6])),
+                         "max_err_over_grad_norm": max(scaled[1e-6]),
+                         "eps_sweep": list(eps_list),
+                         "max_rel_err_by_eps": [max(rel[e]) for e in eps_list],
+                         "max_rel_err_best_eps": max(best_rel),
+                         "max_err_over_grad_norm_best_eps": max(best_scaled)}
         out["gradient"] = g
     elif g_ref is not None:
         out["grad_rel_err_vs_f64"] = float(np.abs(g - g_ref).max() / np.abs(g_ref).max())
@@ -361,8 +463,32 @@ def run_part(args, local_rank):
     else:
         out = {"part": "adjoint", "run": adjoint_bench(stream, args.adj_steps, 0, abi.FP64, n_dirs=0)}
         out["run"].pop("gradient", None)
+        if args.ascent:
+            out["ascent"] = adjoint_ascent(stream, args.adj_steps, args.ascent)
     print(json.dumps(out), flush=True)
     return 0
+
+
+def adjoint_ascent(stream, nsteps, iters):
+    """Projected gradient ascent of the final enstrophy over initial conditions
+    with E = 0.5 and Z = 10 fixed (the extreme-enstrophy search), at 512^2 with
+    the adjoint workload's horizon: Z(T) at the first and the best iterate."""
+    import torch
+    from ns2d import Solver, abi, initial
+    from ns2d import adjoint as nadj
+    p = abi.default_params(nx=ADJ_N, ny=ADJ_N, nu=1e-3, quirks=0, dt=ADJ_DT)
+    s = Solver(p)
+    s.set_stream(stream.cuda_stream)
+    w0 = initial.decaying(ADJ_N, seed=50, k0=4.0, dealias="2/3")
+    t0 = time.perf_counter()
+    wbest, hist = nadj.projected_ascent(s, w0, nsteps, ADJ_DT, iters=iters, e0=0.5, z0=10.0,
+                                       checkpoint_every=ADJ_EVERY)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    out = {"iterations": iters, "J_first": hist[0], "J_best": max(hist), "J_history": hist, "wall_s": wall,
+           "E_best": initial.energy(wbest), "Z0_best": initial.enstrophy(wbest)}
+    s.close()
+    return out
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -445,6 +571,7 @@ def run_gpu(args, rank, world, local_rank):
         # FP32 batched ensemble (same process, same GPU)
         ens_v, ens_ms, ens_grids, ens_launches, ens_z = ensemble_bench(stream, flush, args.ens_steps, args.warmup,
                                                                        rank)
+        ens_err, ens_err_member = ensemble_error(stream, 1000, rank)
         te2 = torch.tensor([ens_ms], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(te2, op=dist.ReduceOp.MAX)
@@ -491,7 +618,9 @@ def run_gpu(args, rank, world, local_rank):
             "ensemble_steps_per_s": ens_total, "ms_per_step": float(te2.item()),
             "equiv_1024_steps_per_s": 4.0 * ens_total, "ratio_vs_fp64_plain": 4.0 * ens_total / value,
             "tuned_grids": {"col": ens_grids[0], "row": ens_grids[1]}, "gpu_launches": int(ens_launches),
-            "enstrophy_sample": ens_z, "launches_per_step": 9,
+            "enstrophy_sample": ens_z, "launches_per_step": ens_launches / max(args.ens_steps, 1),
+            "enstrophy_max_rel_err_vs_fp64": ens_err, "enstrophy_err_member": ens_err_member,
+            "enstrophy_err_steps": 1000,
         }
         line["adjoint"] = {
             "workload": f"gradient of Z(T) w.r.t. w0, {ADJ_N}^2, nu=1e-3, RK4CN dt={ADJ_DT}, {args.adj_steps} steps, "
@@ -500,11 +629,14 @@ def run_gpu(args, rank, world, local_rank):
         }
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, st, el = cpu_reference(1000, 1, threads, budget_s=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
-                                "sample": f"{st} RK4CN steps ({el:.1f} s) of the same {N}^2 workload on the host: "
-                                          "the reference's Solver/src built by oracle/Makefile, FFTW-MPI replaced "
-                                          "by the oracle's OpenMP FFT"}
+        table = cpu_table(threads, runs=5, budget_s=args.cpu_seconds / 6.0)
+        main_row = [r for r in table if r["grid"] == f"{N}x{N}" and r["threads"] == threads][0]
+        line["cpu_baseline"] = {
+            "value": main_row["steps_per_s_median"], "unit": "steps/s", "cores": threads, "kind": "reference",
+            "sample": f"median of 5 timed runs of {main_row['steps_per_run']} RK4CN steps each (after one warm-up "
+                      f"step) of the same {N}^2 workload on {threads} host threads: the reference's Solver/src "
+                      "built by oracle/Makefile, FFTW-MPI replaced by the oracle's OpenMP FFT",
+            "table": table}
     print(json.dumps(line), flush=True)
     s.close()
     return 0
@@ -520,6 +652,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-steps", type=int, default=20)
     ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--ascent", type=int, default=20,
+                    help="--only adjoint: projected-ascent iterations of the final enstrophy (0 = none)")
     ap.add_argument("--only", choices=["plain", "ensemble", "adjoint"], default=None,
                     help="one part alone (profiling runs): plain = the 1024^2 FP64 line without the "
                          "ensemble and adjoint parts; ensemble / adjoint print that part's JSON object")

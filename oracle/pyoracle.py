@@ -132,6 +132,10 @@ class Oracle:
         self.L.oracle_dp5_step(self.h, dt, _ptr(e))
         return float(e[0])
 
+    def set_threads(self, threads):
+        """Host threads of the stand-in FFT from now on."""
+        self.L.ref_set_threads(int(threads))
+
     def rk5dp_step(self, dt, iters):
         """RK5DPStep as the reference writes it, at iteration `iters`; DP_err."""
         return self.L.oracle_rk5dp_step(self.h, dt, iters)
@@ -211,6 +215,7 @@ class RefSolver:
         if variant == "ab4":
             L.ref_ab4_step.argtypes = [C.c_double, C.c_int]
         L.ref_compute_forcing.argtypes = [C.c_double]
+        L.ref_set_threads.argtypes = [C.c_int]
         L.ref_apply_dealiasing.argtypes = [_dp, C.c_int]
         L.ref_force_conjugacy.argtypes = [_dp]
         for f in ("ref_get_max_vort", "ref_get_max_vel", "ref_w_max_init"):
@@ -263,6 +268,10 @@ class RefSolver:
 
     def ab4_step(self, dt, iters):
         self.L.ref_ab4_step(dt, iters)
+
+    def set_threads(self, threads):
+        """Host threads of the stand-in FFT from now on."""
+        self.L.ref_set_threads(int(threads))
 
     def rk5dp_step(self, dt, iters):
         """RK5DPStep at iteration `iters` (variant "dp5"); returns DP_err."""

@@ -145,6 +145,9 @@ void ref_get_k(int* kx, int* ky) {
 int ref_hyper_visc_flag(void) { return sys_vars->HYPER_VISC_FLAG; }
 void ref_set_hyper_visc_flag(int f) { sys_vars->HYPER_VISC_FLAG = f; }
 void ref_compute_forcing(double dt) { ComputeForcing(dt); }
+/* Host threads of the stand-in FFT (FFTW-MPI's place); the reference's own
+   loops stay single-threaded, as in one MPI rank. */
+void ref_set_threads(int threads) { offt_set_threads(threads); }
 
 #if defined(__RK4) || defined(__RK4CN) || defined(__AB4)
 void ref_rk4_step(double dt) { RK4Step(dt, g_N, sys_vars->local_Nx, &g_int); }

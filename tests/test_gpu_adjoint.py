@@ -103,6 +103,43 @@ def test_central_differences():
         assert abs(fd - ar.wdot(g, d)) <= 1e-6 * abs(fd)
 
 
+def test_central_differences_512():
+    """The gradient workload's grid and step (512^2, nu = 1e-3, dt = 5e-4,
+    checkpoints every 50 steps, w0 with E = 0.5 and Z = 10) over a 200-step
+    horizon, 16 seeded directions, central differences with eps = 1e-5 and
+    1e-6 (|d|_W = |w0|_W), the better of the two kept.  Enforced:
+    |FD - <g, d>_W| <= 1e-9 |g|_W |d|_W on every direction (a difference of two
+    objective values carries about 1e-16 J / eps of rounding, which swamps the
+    relative error of a direction nearly orthogonal to g), and the relative
+    error <= 1e-6 on directions with |<g, d>_W| >= 1e-2 |g|_W |d|_W."""
+    n, steps, dt = 512, 200, 5e-4
+    p = _params(n)
+    w0 = nadj.project(initial.decaying(n, 50, k0=4.0, dealias="2/3"), 0.5, 10.0)
+    s = Solver(p)
+    s.set_w_hat(w0)
+    J, g = s.adjoint_gradient(steps, dt, 50)
+    gn = np.sqrt(ar.wdot(g, g))
+    wn = np.sqrt(ar.wdot(w0, w0))
+    rng = np.random.default_rng(900)
+    for _ in range(16):
+        d = initial.dealias_23(initial.hermitian(rng.standard_normal(w0.shape) + 1j * rng.standard_normal(w0.shape)))
+        d *= wn / np.sqrt(ar.wdot(d, d))
+        ad = ar.wdot(g, d)
+        errs = []
+        for eps in (1e-5, 1e-6):
+            vals = []
+            for sgn in (1.0, -1.0):
+                s.set_w_hat(w0 + sgn * eps * d)
+                s.step_n(steps, dt)
+                vals.append(s.objective(abi.OBJ_ENSTROPHY))
+            errs.append(abs((vals[0] - vals[1]) / (2 * eps) - ad))
+        err = min(errs)
+        assert err <= 1e-9 * gn * wn, (err / (gn * wn), ad / (gn * wn))
+        if abs(ad) >= 1e-2 * gn * wn:
+            assert err <= 1e-6 * abs(ad), (err / abs(ad), ad / (gn * wn))
+    s.close()
+
+
 def test_checkpoint_interval_is_bitwise_neutral():
     n, steps, dt = 64, 12, 2e-3
     p = _params(n)
