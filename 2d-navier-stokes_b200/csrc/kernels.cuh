@@ -171,12 +171,20 @@ struct ColSmem {
     static constexpr size_t bytes() { return sizeof(C) * (size_t)(2 * FFT + PRE); }
 };
 
-// 1/k^2 for the velocity spectra: the correctly rounded reciprocal (the same
-// value as 1.0/k2) in FP64, single precision in the FP32 form.
+// 1/k^2 for the velocity spectra.  FP64: Newton-Raphson for the reciprocal,
+// r <- r + r (1 - k2 r), twice from the single-precision reciprocal (k2 < 2^24
+// is exact in FP32, the seed's relative error is below 2^-23, so two steps
+// leave about one rounding of FP64); single precision in the FP32 form.
 template <typename Real>
 __device__ __forceinline__ Real inv_k2(int k2);
 template <>
-__device__ __forceinline__ double inv_k2<double>(int k2) { return __drcp_rn((double)k2); }
+__device__ __forceinline__ double inv_k2<double>(int k2) {
+    const double d = (double)k2;
+    double r = (double)__frcp_rn((float)k2);
+    r = fma(r, fma(-d, r, 1.0), r);
+    r = fma(r, fma(-d, r, 1.0), r);
+    return r;
+}
 template <>
 __device__ __forceinline__ float inv_k2<float>(int k2) { return __frcp_rn((float)k2); }
 
