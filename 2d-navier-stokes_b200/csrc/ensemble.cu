@@ -32,9 +32,12 @@ struct ns2d_ensemble {
     // device memory
     std::vector<void*> allocs;
     void* members = nullptr;      // EnsMember<Real>[n]
-    EnsItem* col_items = nullptr;
-    EnsItem* row_items = nullptr;
-    int n_col_items = 0, n_row_items = 0;
+    // work items of each block-size choice (kEnsThreadChoices) and the choice
+    // each pass uses
+    EnsItem* col_items[2] = {nullptr, nullptr};
+    EnsItem* row_items[2] = {nullptr, nullptr};
+    int n_col_items[2] = {0, 0}, n_row_items[2] = {0, 0};
+    int col_var = 0, row_var = 0;
     int* status = nullptr;
     double* ddiag = nullptr;
     std::vector<void*> state, nl, acc, tw;
@@ -48,8 +51,8 @@ struct ns2d_ensemble {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double graph_dt = -1.0;
-    int graph_col_grid = 0, graph_row_grid = 0;
-    size_t col_smem = 0, row_smem = 0;
+    int graph_col_grid = 0, graph_row_grid = 0, graph_col_var = -1, graph_row_var = -1;
+    size_t col_smem[2] = {0, 0}, row_smem[2] = {0, 0};
     int nsm = 148;
 };
 
@@ -78,23 +81,71 @@ bool ens_size_ok(int n) {
     }
 }
 
-int ens_col_tc(int n) {
+// Column tile width and rows per row block of a member of size n under block
+// size kEnsThreadChoices[v].
+int ens_col_tc(int n, int v) {
     switch (n) {
 #define NS2D_ENS_TC(NN) \
-    case NN: return EnsShape<NN>::TC;
+    case NN: return v == 0 ? EnsShape<NN, kEnsThreadChoices[0]>::TC : EnsShape<NN, kEnsThreadChoices[1]>::TC;
         NS2D_ENS_SIZES(NS2D_ENS_TC)
 #undef NS2D_ENS_TC
         default: return 1;
     }
 }
-int ens_row_tc(int n) {
+int ens_row_tc(int n, int v) {
     switch (n) {
 #define NS2D_ENS_RT(NN) \
-    case NN: return 2 * EnsShape<NN>::PAIRS;
+    case NN: return 2 * (v == 0 ? EnsShape<NN, kEnsThreadChoices[0]>::PAIRS : EnsShape<NN, kEnsThreadChoices[1]>::PAIRS);
         NS2D_ENS_SIZES(NS2D_ENS_RT)
 #undef NS2D_ENS_RT
         default: return 2;
     }
+}
+
+template <typename Real, int V>
+cudaError_t ens_set_smem(ns2d_ensemble* e) {
+    constexpr int TH = kEnsThreadChoices[V];
+    e->col_smem[V] = EnsSmem<Real, TH>::col();
+    e->row_smem[V] = EnsSmem<Real, TH>::row();
+    cudaError_t r = cudaSuccess;
+    auto set = [&](const void* f, size_t b) {
+        if (r == cudaSuccess) r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+    };
+    set((const void*)ens_col_kernel<Real, COL_P1, TH>, e->col_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_STAGE, TH>, e->col_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_FINAL, TH>, e->col_smem[V]);
+    set((const void*)ens_row_kernel<Real, TH>, e->row_smem[V]);
+    return r;
+}
+
+// Blocks per SM of the choice's column and row kernels.
+template <typename Real, int V>
+void ens_occupancy(const ns2d_ensemble* e, int* col_per_sm, int* row_per_sm) {
+    constexpr int TH = kEnsThreadChoices[V];
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(col_per_sm, ens_col_kernel<Real, COL_STAGE, TH>, TH, e->col_smem[V]);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(row_per_sm, ens_row_kernel<Real, TH>, TH, e->row_smem[V]);
+}
+
+template <typename Real, int MODE>
+void ens_launch_col(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
+    const int v = e->col_var;
+    if (v == 0)
+        ens_col_kernel<Real, MODE, kEnsThreadChoices[0]><<<e->col_grid, kEnsThreadChoices[0], e->col_smem[0], e->stream>>>(
+            mb, e->col_items[0], e->n_col_items[0], st);
+    else
+        ens_col_kernel<Real, MODE, kEnsThreadChoices[1]><<<e->col_grid, kEnsThreadChoices[1], e->col_smem[1], e->stream>>>(
+            mb, e->col_items[1], e->n_col_items[1], st);
+}
+
+template <typename Real>
+void ens_launch_row(ns2d_ensemble* e, const EnsMember<Real>* mb) {
+    const int v = e->row_var;
+    if (v == 0)
+        ens_row_kernel<Real, kEnsThreadChoices[0]><<<e->row_grid, kEnsThreadChoices[0], e->row_smem[0], e->stream>>>(
+            mb, e->row_items[0], e->n_row_items[0], e->status);
+    else
+        ens_row_kernel<Real, kEnsThreadChoices[1]><<<e->row_grid, kEnsThreadChoices[1], e->row_smem[1], e->stream>>>(
+            mb, e->row_items[1], e->n_row_items[1], e->status);
 }
 
 template <typename Real>
@@ -185,8 +236,6 @@ ns2d_status create_t(ns2d_ensemble* e) {
         mb.col0[0] = (C*)c0[0];
         mb.col0[1] = (C*)c0[1];
         mb.n = n;
-        mb.col_tiles = (nyf + ens_col_tc(n) - 1) / ens_col_tc(n);
-        mb.row_blocks = n / ens_row_tc(n);
     }
     ECK(e, alloc(sizeof(EnsMember<Real>) * e->n, &e->members));
     ECK(e, cudaMemcpyAsync(e->members, hm.data(), sizeof(EnsMember<Real>) * e->n, cudaMemcpyHostToDevice, e->stream));
@@ -197,36 +246,37 @@ ns2d_status create_t(ns2d_ensemble* e) {
     ECK(e, alloc(sizeof(double) * (DG_N + 8 * (size_t)nspect_max), (void**)&e->ddiag));
     ECK(e, cudaFuncSetAttribute((const void*)diag_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(sizeof(double) * (8 * (size_t)nspect_max + DG_N * 8))));
-    // work items, largest grids first (longest-processing-time order)
-    std::vector<EnsItem> ci, ri;
+    // work items of each block-size choice, largest grids first
+    // (longest-processing-time order)
     std::vector<int> order(e->n);
     for (int m = 0; m < e->n; ++m) order[m] = m;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return e->sizes[x] > e->sizes[y]; });
-    for (int m : order) {
-        for (int t = 0; t < hm[m].col_tiles; ++t) ci.push_back({m, t});
-        for (int r = 0; r < hm[m].row_blocks; ++r) ri.push_back({m, r});
+    for (int v = 0; v < 2; ++v) {
+        std::vector<EnsItem> ci, ri;
+        for (int m : order) {
+            const int n = e->sizes[m];
+            const int tiles = (n / 2 + 1 + ens_col_tc(n, v) - 1) / ens_col_tc(n, v);
+            for (int t = 0; t < tiles; ++t) ci.push_back({m, t});
+            for (int r = 0; r < n / ens_row_tc(n, v); ++r) ri.push_back({m, r});
+        }
+        e->n_col_items[v] = (int)ci.size();
+        e->n_row_items[v] = (int)ri.size();
+        ECK(e, alloc(sizeof(EnsItem) * ci.size(), (void**)&e->col_items[v]));
+        ECK(e, alloc(sizeof(EnsItem) * ri.size(), (void**)&e->row_items[v]));
+        ECK(e, cudaMemcpyAsync(e->col_items[v], ci.data(), sizeof(EnsItem) * ci.size(), cudaMemcpyHostToDevice, e->stream));
+        ECK(e, cudaMemcpyAsync(e->row_items[v], ri.data(), sizeof(EnsItem) * ri.size(), cudaMemcpyHostToDevice, e->stream));
     }
-    e->n_col_items = (int)ci.size();
-    e->n_row_items = (int)ri.size();
-    ECK(e, alloc(sizeof(EnsItem) * ci.size(), (void**)&e->col_items));
-    ECK(e, alloc(sizeof(EnsItem) * ri.size(), (void**)&e->row_items));
-    ECK(e, cudaMemcpyAsync(e->col_items, ci.data(), sizeof(EnsItem) * ci.size(), cudaMemcpyHostToDevice, e->stream));
-    ECK(e, cudaMemcpyAsync(e->row_items, ri.data(), sizeof(EnsItem) * ri.size(), cudaMemcpyHostToDevice, e->stream));
-    e->col_smem = EnsSmem<Real>::col();
-    e->row_smem = EnsSmem<Real>::row();
-    ECK(e, cudaFuncSetAttribute((const void*)ens_col_kernel<Real, COL_P1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->col_smem));
-    ECK(e, cudaFuncSetAttribute((const void*)ens_col_kernel<Real, COL_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->col_smem));
-    ECK(e, cudaFuncSetAttribute((const void*)ens_col_kernel<Real, COL_FINAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->col_smem));
-    ECK(e, cudaFuncSetAttribute((const void*)ens_row_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->row_smem));
+    ECK(e, (ens_set_smem<Real, 0>(e)));
+    ECK(e, (ens_set_smem<Real, 1>(e)));
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, dev);
-    // default persistent grids: every item in one wave where it fits
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_col_kernel<Real, COL_STAGE>, kEnsThreads, e->col_smem);
-    e->col_grid = std::max(1, std::min(e->n_col_items, e->nsm * std::max(1, per_sm)));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_row_kernel<Real>, kEnsThreads, e->row_smem);
-    e->row_grid = std::max(1, std::min(e->n_row_items, e->nsm * std::max(1, per_sm)));
+    // default: 256-thread blocks, persistent grids with every item in one wave where it fits
+    int col_per_sm = 0, row_per_sm = 0;
+    ens_occupancy<Real, 0>(e, &col_per_sm, &row_per_sm);
+    e->col_var = e->row_var = 0;
+    e->col_grid = std::max(1, std::min(e->n_col_items[0], e->nsm * std::max(1, col_per_sm)));
+    e->row_grid = std::max(1, std::min(e->n_row_items[0], e->nsm * std::max(1, row_per_sm)));
     ECK(e, cudaStreamSynchronize(e->stream));
     return NS2D_OK;
 }
@@ -259,20 +309,20 @@ ns2d_status step_t(ns2d_ensemble* e, double dt) {
     st.conj_quirk = (e->p.quirks & NS2D_QUIRK_CONJ_STATE) ? 1 : 0;
     st.status = e->status;
     st.stage = 0;
-    ens_col_kernel<Real, COL_P1><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+    ens_launch_col<Real, COL_P1>(e, mb, st);
     e->launches++;
     for (int s = 1; s <= 4; ++s) {
-        ens_row_kernel<Real><<<e->row_grid, kEnsThreads, e->row_smem, e->stream>>>(mb, e->row_items, e->n_row_items, e->status);
+        ens_launch_row<Real>(e, mb);
         e->launches++;
         st.stage = s;
         st.b_cur = explicit_rk4 ? B_ex[s - 1] : B_cn[s - 1];
         if (s < 4) {
             st.a_next = A[s - 1];
             st.first = (s == 1);
-            ens_col_kernel<Real, COL_STAGE><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+            ens_launch_col<Real, COL_STAGE>(e, mb, st);
         } else {
             st.scheme = explicit_rk4 ? 1 : 0;
-            ens_col_kernel<Real, COL_FINAL><<<e->col_grid, kEnsThreads, e->col_smem, e->stream>>>(mb, e->col_items, e->n_col_items, st);
+            ens_launch_col<Real, COL_FINAL>(e, mb, st);
         }
         e->launches++;
     }
@@ -287,7 +337,8 @@ ns2d_status step_t(ns2d_ensemble* e, double dt) {
 // after an eager step at this dt, so the CN tables exist and the operator
 // branch is settled: capturing records exactly the 9 pass launches.
 ns2d_status ensure_graph(ns2d_ensemble* e, double dt) {
-    if (e->exec && e->graph_dt == dt && e->graph_col_grid == e->col_grid && e->graph_row_grid == e->row_grid)
+    if (e->exec && e->graph_dt == dt && e->graph_col_grid == e->col_grid && e->graph_row_grid == e->row_grid &&
+        e->graph_col_var == e->col_var && e->graph_row_var == e->row_var)
         return NS2D_OK;
     if (e->exec) {
         cudaGraphExecDestroy(e->exec);
@@ -315,6 +366,8 @@ ns2d_status ensure_graph(ns2d_ensemble* e, double dt) {
     e->graph_dt = dt;
     e->graph_col_grid = e->col_grid;
     e->graph_row_grid = e->row_grid;
+    e->graph_col_var = e->col_var;
+    e->graph_row_var = e->row_var;
     return NS2D_OK;
 }
 
@@ -526,41 +579,83 @@ ns2d_status ns2d_ensemble_measurables(ns2d_ensemble* e, int32_t member, ns2d_mea
 
 ns2d_status ns2d_ensemble_set_grids(ns2d_ensemble* e, int32_t col_grid, int32_t row_grid) {
     if (!e || col_grid < 1 || row_grid < 1) return NS2D_ERR_INVALID;
-    e->col_grid = std::min(col_grid, e->n_col_items);
-    e->row_grid = std::min(row_grid, e->n_row_items);
+    e->col_grid = std::min(col_grid, e->n_col_items[e->col_var]);
+    e->row_grid = std::min(row_grid, e->n_row_items[e->row_var]);
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_ensemble_set_shape(ns2d_ensemble* e, const ns2d_ensemble_shape* sh) {
+    if (!e || !sh || sh->col_grid < 1 || sh->row_grid < 1) return NS2D_ERR_INVALID;
+    int cv = -1, rv = -1;
+    for (int v = 0; v < 2; ++v) {
+        if (sh->col_threads == kEnsThreadChoices[v]) cv = v;
+        if (sh->row_threads == kEnsThreadChoices[v]) rv = v;
+    }
+    if (cv < 0 || rv < 0) return NS2D_ERR_INVALID;
+    e->col_var = cv;
+    e->row_var = rv;
+    e->col_grid = std::min(sh->col_grid, e->n_col_items[cv]);
+    e->row_grid = std::min(sh->row_grid, e->n_row_items[rv]);
+    return NS2D_OK;
+}
+
+ns2d_status ns2d_ensemble_get_shape(const ns2d_ensemble* e, ns2d_ensemble_shape* sh) {
+    if (!e || !sh) return NS2D_ERR_INVALID;
+    sh->col_threads = kEnsThreadChoices[e->col_var];
+    sh->col_grid = e->col_grid;
+    sh->row_threads = kEnsThreadChoices[e->row_var];
+    sh->row_grid = e->row_grid;
+    sh->col_items = e->n_col_items[e->col_var];
+    sh->row_items = e->n_row_items[e->row_var];
     return NS2D_OK;
 }
 
 ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, int32_t* row_grid) {
     if (!e) return NS2D_ERR_INVALID;
     cudaSetDevice(e->p.device);
-    // Autotuner: the persistent grid of each pass, as a multiple of the SM
-    // count (1..8 blocks per SM, capped by the item count), chosen by timing
-    // full steps; the column and row grids are tuned one after the other.
-    // Steps taken here advance the members; callers re-set their states.
+    // Autotuner: for each pass (the four column launches, then the four row
+    // launches of a step), the block size -- which sets the tile shape: ky
+    // columns per column tile and row pairs per row block of every member --
+    // and the persistent grid as a multiple of the SM count (1..8 blocks per
+    // SM, capped by the item count), chosen by timing full steps.  Steps taken
+    // here advance the members; callers re-set their states.
     const int saved_hyper = e->hyper_flag;
     EDISPATCH(e, step_t, e, dt);  // settle tables and the operator branch
     cudaStreamSynchronize(e->stream);
     const int mults[] = {1, 2, 3, 4, 6, 8};
-    int best_c = e->col_grid, best_r = e->row_grid;
+    int best_cv = e->col_var, best_rv = e->row_var, best_c = e->col_grid, best_r = e->row_grid;
     double best = time_steps(e, dt, 3);
     for (int pass = 0; pass < 2; ++pass) {
-        for (int k : mults) {
-            const int g = std::min(k * e->nsm, pass == 0 ? e->n_col_items : e->n_row_items);
-            if (pass == 0) e->col_grid = g;
-            else e->row_grid = g;
-            const double ms = time_steps(e, dt, 3);
-            if (ms < best) {
-                best = ms;
-                if (pass == 0) best_c = g;
-                else best_r = g;
+        for (int v = 0; v < 2; ++v) {
+            for (int k : mults) {
+                if (pass == 0) {
+                    e->col_var = v;
+                    e->col_grid = std::min(k * e->nsm, e->n_col_items[v]);
+                } else {
+                    e->row_var = v;
+                    e->row_grid = std::min(k * e->nsm, e->n_row_items[v]);
+                }
+                const double ms = time_steps(e, dt, 3);
+                if (ms < best) {
+                    best = ms;
+                    if (pass == 0) {
+                        best_cv = v;
+                        best_c = e->col_grid;
+                    } else {
+                        best_rv = v;
+                        best_r = e->row_grid;
+                    }
+                }
             }
-            if (pass == 0) e->col_grid = best_c;
-            else e->row_grid = best_r;
+        }
+        if (pass == 0) {
+            e->col_var = best_cv;
+            e->col_grid = best_c;
+        } else {
+            e->row_var = best_rv;
+            e->row_grid = best_r;
         }
     }
-    e->col_grid = best_c;
-    e->row_grid = best_r;
     e->hyper_flag = saved_hyper;
     cudaError_t r = cudaGetLastError();
     if (r != cudaSuccess) return efail(e, NS2D_ERR_CUDA, cudaGetErrorString(r));

@@ -9,17 +9,20 @@
 
 namespace ns2d {
 
-// Block size of the ensemble kernels (every member size), and the tile shapes
-// it gives.  256 threads measured 12 % faster than 128 on the 64-member FP32
-// benchmark ensemble: the 512^2 members' column tiles grow from 2 to 4 columns
-// (32 B per row access in FP32), the 128^2 / 256^2 ones from 8 to 16.
-constexpr int kEnsThreads = 256;
-template <int N>
+// Block sizes of the ensemble kernels (one per launch, every member size), and
+// the tile shapes they give: a block of THREADS threads covers THREADS / T
+// ky columns of a member in a column pass and THREADS / (2 T) row pairs in a
+// row pass (T = the threads of one transform of that size).  The autotuner
+// picks the block size of each pass; 256 threads measured 12 % faster than
+// 128 on the 64-member FP32 benchmark ensemble (the 512^2 members' column
+// tiles grow from 2 to 4 columns, the 128^2 / 256^2 ones from 8 to 16).
+constexpr int kEnsThreadChoices[2] = {256, 128};
+template <int N, int THREADS>
 struct EnsShape {
     static constexpr int T = Plan<N>::T;
-    static constexpr int TC = kEnsThreads / T;          // columns per column tile
-    static constexpr int PAIRS = kEnsThreads / (2 * T);  // row pairs per row block
-    static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= kEnsThreads / 2");
+    static constexpr int TC = THREADS / T;          // columns per column tile
+    static constexpr int PAIRS = THREADS / (2 * T);  // row pairs per row block
+    static_assert(TC >= 1 && PAIRS >= 1, "ensemble sizes need T <= THREADS / 2");
 };
 
 #define NS2D_ENS_SIZES(X) X(64) X(128) X(256) X(512)
@@ -30,7 +33,6 @@ struct EnsMember {
     RowArgs<Real> row;
     typename Cx<Real>::T* col0[2];        // column 0 of successive stage inputs
     int n;
-    int col_tiles, row_blocks;
 };
 
 struct EnsItem {
@@ -73,16 +75,16 @@ __device__ __forceinline__ void ens_apply_stage(ColArgs<Real>& a, const EnsMembe
     }
 }
 
-// Resident blocks per SM the ensemble kernels are compiled for: two in FP32
-// (at most 128 registers a thread), the register need of one FP64 body
-// otherwise.
-template <typename Real>
+// Resident blocks per SM the ensemble kernels are compiled for: at most 128
+// registers a thread in FP32 (two 256-thread or four 128-thread blocks), the
+// register need of one FP64 body otherwise.
+template <typename Real, int THREADS>
 struct EnsMinBlocks {
-    static constexpr int value = sizeof(Real) == 4 ? 2 : 1;
+    static constexpr int value = sizeof(Real) == 4 ? 512 / THREADS : 256 / THREADS;
 };
 
-template <typename Real, int MODE>
-__global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
+template <typename Real, int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value)) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, EnsStage st) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(st.status)) return;
@@ -92,9 +94,9 @@ __global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_co
         ColArgs<Real> a = mb.col;
         ens_apply_stage(a, mb, st);
         switch (mb.n) {
-#define NS2D_ENS_COL(NN)                                                         \
-    case NN:                                                                     \
-        col_body<Real, NN, EnsShape<NN>::TC, MODE>(a, item.tile, smraw);         \
+#define NS2D_ENS_COL(NN)                                                                  \
+    case NN:                                                                              \
+        col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE>(a, item.tile, smraw);         \
         break;
             NS2D_ENS_SIZES(NS2D_ENS_COL)
 #undef NS2D_ENS_COL
@@ -103,8 +105,8 @@ __global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_co
     }
 }
 
-template <typename Real>
-__global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
+template <typename Real, int THREADS>
+__global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value)) ens_row_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, int* status) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(status)) return;
@@ -112,9 +114,9 @@ __global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_ro
         const EnsItem item = items[it];
         const EnsMember<Real>& mb = members[item.member];
         switch (mb.n) {
-#define NS2D_ENS_ROW(NN)                                                         \
-    case NN:                                                                     \
-        row_body<Real, NN, EnsShape<NN>::PAIRS>(mb.row, item.tile, smraw);       \
+#define NS2D_ENS_ROW(NN)                                                                  \
+    case NN:                                                                              \
+        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS>(mb.row, item.tile, smraw);       \
         break;
             NS2D_ENS_SIZES(NS2D_ENS_ROW)
 #undef NS2D_ENS_ROW
@@ -123,18 +125,23 @@ __global__ void __launch_bounds__(kEnsThreads, EnsMinBlocks<Real>::value) ens_ro
     }
 }
 
-template <typename Real>
+template <typename Real, int THREADS>
 struct EnsSmem {
     static size_t col() {
         size_t m = 0;
-#define NS2D_ENS_CS(NN) m = m > ColSmem<Real, NN, EnsShape<NN>::TC>::bytes() ? m : ColSmem<Real, NN, EnsShape<NN>::TC>::bytes();
+#define NS2D_ENS_CS(NN)                                                                       \
+    m = m > ColSmem<Real, NN, EnsShape<NN, THREADS>::TC>::bytes() ? m                         \
+                                                                  : ColSmem<Real, NN, EnsShape<NN, THREADS>::TC>::bytes();
         NS2D_ENS_SIZES(NS2D_ENS_CS)
 #undef NS2D_ENS_CS
         return m;
     }
     static size_t row() {
         size_t m = 0;
-#define NS2D_ENS_RS(NN) m = m > RowSmem<Real, NN, 2 * EnsShape<NN>::PAIRS>::bytes() ? m : RowSmem<Real, NN, 2 * EnsShape<NN>::PAIRS>::bytes();
+#define NS2D_ENS_RS(NN)                                                                              \
+    m = m > RowSmem<Real, NN, 2 * EnsShape<NN, THREADS>::PAIRS>::bytes()                             \
+            ? m                                                                                      \
+            : RowSmem<Real, NN, 2 * EnsShape<NN, THREADS>::PAIRS>::bytes();
         NS2D_ENS_SIZES(NS2D_ENS_RS)
 #undef NS2D_ENS_RS
         return m;

@@ -10,6 +10,16 @@ from ._lib import NS2DError, load
 _dp = C.POINTER(C.c_double)
 
 
+class Shape(C.Structure):
+    """struct ns2d_ensemble_shape: block size and persistent grid of the column
+    and of the row passes, and (out) the item counts of those shapes."""
+    _fields_ = [(n, C.c_int32) for n in ("col_threads", "col_grid", "row_threads", "row_grid", "col_items",
+                                          "row_items")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 def _sig(L):
     H = C.c_void_p
     sig = {
@@ -25,6 +35,8 @@ def _sig(L):
         "ns2d_ensemble_measurables": (C.c_int, [H, C.c_int32, C.POINTER(abi.Measures)]),
         "ns2d_ensemble_tune": (C.c_int, [H, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "ns2d_ensemble_set_grids": (C.c_int, [H, C.c_int32, C.c_int32]),
+        "ns2d_ensemble_set_shape": (C.c_int, [H, C.POINTER(Shape)]),
+        "ns2d_ensemble_get_shape": (C.c_int, [H, C.POINTER(Shape)]),
         "ns2d_ensemble_set_stream": (C.c_int, [H, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
@@ -94,6 +106,17 @@ class Ensemble:
 
     def set_grids(self, col_grid, row_grid):
         self._ck(self.L.ns2d_ensemble_set_grids(self.h, col_grid, row_grid))
+
+    @property
+    def shape(self):
+        """Launch shape of the passes (ns2d_ensemble_get_shape) as a dict."""
+        sh = Shape()
+        self._ck(self.L.ns2d_ensemble_get_shape(self.h, C.byref(sh)))
+        return sh.as_dict()
+
+    def set_shape(self, col_threads, col_grid, row_threads, row_grid):
+        sh = Shape(col_threads=col_threads, col_grid=col_grid, row_threads=row_threads, row_grid=row_grid)
+        self._ck(self.L.ns2d_ensemble_set_shape(self.h, C.byref(sh)))
 
     def set_stream(self, ptr):
         self._ck(self.L.ns2d_ensemble_set_stream(self.h, C.c_void_p(ptr)))

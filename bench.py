@@ -316,8 +316,9 @@ def ensemble_bench(stream, flush, steps, warmup, rank):
     """The uneven-ensemble workload: 64 members (32 x 128^2, 24 x 256^2, 8 x 512^2), FP32
     RK4CN, nu = 1e-3, decaying spectra with k0 drawn from {4, 6, 8}; every pass
     of a step is one launch for all members, the step replayed from a CUDA
-    graph, persistent grids picked by the autotuner.  Returns ensemble steps/s
-    (device time, L2 flushed between steps) and the tuned grids."""
+    graph, block sizes (tile shapes) and persistent grids picked by the
+    autotuner.  Returns ensemble steps/s (device time, L2 flushed between
+    steps) and the tuned launch shape."""
     import torch
     from ns2d import Ensemble, abi, initial
     p = abi.default_params(nu=1e-3, dt=ENS_DT, precision=abi.FP32)
@@ -326,7 +327,8 @@ def ensemble_bench(stream, flush, steps, warmup, rank):
     rng = np.random.default_rng(100 + rank)
     ics = [initial.decaying(n, seed=1000 * rank + m, k0=float(rng.choice([4, 6, 8])), dealias="2/3")
            for m, n in enumerate(ENS_SIZES)]
-    grids = e.tune(ENS_DT)
+    e.tune(ENS_DT)
+    grids = e.shape
     for m, w in enumerate(ics):
         e.set_w_hat(m, w)
     e.step_async(warmup, ENS_DT)
@@ -467,7 +469,7 @@ def run_part(args, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     if args.only == "ensemble":
         v, ms, grids, launches, z = ensemble_bench(stream, flush, args.ens_steps, args.warmup, 0)
-        out = {"part": "ensemble", "ensemble_steps_per_s": v, "ms_per_step": ms, "tuned_grids": grids,
+        out = {"part": "ensemble", "ensemble_steps_per_s": v, "ms_per_step": ms, "tuned_shape": grids,
                "gpu_launches": launches, "enstrophy_sample": z}
     else:
         out = {"part": "adjoint", "run": adjoint_bench(stream, args.adj_steps, 0, abi.FP64, n_dirs=0)}
@@ -638,7 +640,7 @@ def run_gpu(args, rank, world, local_rank):
             "workload": "ensemble 32x128^2 + 24x256^2 + 8x512^2 (4 x 1024^2 points), FP32 RK4CN, nu=1e-3, dt=1e-3",
             "ensemble_steps_per_s": ens_total, "ms_per_step": float(te2.item()),
             "equiv_1024_steps_per_s": 4.0 * ens_total, "ratio_vs_fp64_plain": 4.0 * ens_total / value,
-            "tuned_grids": {"col": ens_grids[0], "row": ens_grids[1]}, "gpu_launches": int(ens_launches),
+            "tuned_shape": ens_grids, "gpu_launches": int(ens_launches),
             "enstrophy_sample": ens_z, "launches_per_step": ens_launches / max(args.ens_steps, 1),
             "enstrophy_max_rel_err_vs_fp64": ens_err, "enstrophy_err_member": ens_err_member,
             "enstrophy_err_steps": 1000,

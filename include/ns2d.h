@@ -394,10 +394,27 @@ ns2d_status ns2d_ensemble_step_async(ns2d_ensemble* e, int32_t nsteps, double dt
 ns2d_status ns2d_ensemble_check(ns2d_ensemble* e);
 /* Totals of ComputeSystemMeasurables for one member, flux terms set to 0. */
 ns2d_status ns2d_ensemble_measurables(ns2d_ensemble* e, int32_t member, ns2d_measures* out);
-/* Autotuner: picks the persistent grid of the column and row passes (1..8
-   blocks per SM) by timing steps at dt.  It advances the members. */
+/* Autotuner: picks, for the column and for the row passes, the block size
+   (the tile shape, ns2d_ensemble_shape below) and the persistent grid (1..8
+   blocks per SM) by timing steps at dt; returns the grids.  It advances the
+   members.  ns2d_ensemble_set_grids keeps the block sizes. */
 ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, int32_t* row_grid);
 ns2d_status ns2d_ensemble_set_grids(ns2d_ensemble* e, int32_t col_grid, int32_t row_grid);
+/* Launch shape of the ensemble's passes: block size of the column and of the
+   row launches (256 or 128 threads; it sets the tile shape -- ky columns per
+   column tile and row pairs per row block of every member, threads / T and
+   threads / 2T with T the threads of one transform of the member's size) and
+   their persistent grids; the item counts of the chosen shapes are reported.
+   ns2d_ensemble_tune picks all four by timing steps (no reference
+   counterpart: the reference runs sweeps as separate processes,
+   Solver/run_solver.py:270-292). */
+typedef struct ns2d_ensemble_shape {
+    int32_t col_threads, col_grid;
+    int32_t row_threads, row_grid;
+    int32_t col_items, row_items;   /* out only */
+} ns2d_ensemble_shape;
+ns2d_status ns2d_ensemble_set_shape(ns2d_ensemble* e, const ns2d_ensemble_shape* shape);
+ns2d_status ns2d_ensemble_get_shape(const ns2d_ensemble* e, ns2d_ensemble_shape* shape);
 ns2d_status ns2d_ensemble_set_stream(ns2d_ensemble* e, void* cuda_stream);
 
 /* Execution control. */

@@ -95,3 +95,30 @@ def test_autotuner_and_graph_replay_keep_results():
         assert rel_err(e.get_w_hat(m), ref.get_w_hat(m)) <= 1e-15
     e.close()
     ref.close()
+
+
+@pytest.mark.parametrize("col_threads,row_threads", [(128, 128), (128, 256), (256, 128)])
+def test_block_size_choices_keep_results(col_threads, row_threads):
+    """The autotuner's tile-shape choices (block size of the column and of the
+    row launches) change only how members are cut into tiles: every member
+    equals the default 256-thread shape's result."""
+    sizes = [64, 512, 128, 256]
+    p = abi.default_params(nu=1e-3, dt=1e-3)
+    ics = _ics(sizes, seed0=90)
+    ref = Ensemble(p, sizes)
+    e = Ensemble(p, sizes)
+    sh = e.shape
+    assert (sh["col_threads"], sh["row_threads"]) == (256, 256)
+    e.set_shape(col_threads, 2 * 148, row_threads, 3 * 148)
+    sh = e.shape
+    assert (sh["col_threads"], sh["row_threads"]) == (col_threads, row_threads)
+    assert sh["col_grid"] <= sh["col_items"] and sh["row_grid"] <= sh["row_items"]
+    for m, w in enumerate(ics):
+        ref.set_w_hat(m, w)
+        e.set_w_hat(m, w)
+    ref.step_n(5, 1e-3)
+    e.step_n(5, 1e-3)
+    for m in range(len(sizes)):
+        assert rel_err(e.get_w_hat(m), ref.get_w_hat(m)) <= 1e-15, m
+    e.close()
+    ref.close()
