@@ -38,6 +38,16 @@ struct ns2d_ensemble {
     EnsItem* row_items[2] = {nullptr, nullptr};
     int n_col_items[2] = {0, 0}, n_row_items[2] = {0, 0};
     int col_var = 0, row_var = 0;
+    // one persistent launch per RK stage (ens_stage_kernel): its task list
+    // (first-pass column tiles, then row blocks, then column tiles), the work
+    // and completion counters, the tasks' input counts, smem and grid
+    bool fused = false;
+    EnsTask* tasks = nullptr;
+    int n_tasks = 0, n_p1_tasks = 0;
+    int* sync = nullptr;          // [4] heads, then [5][n] completion counters
+    int* need = nullptr;          // [n][2]
+    size_t stage_smem = 0;
+    int stage_grid = 0, stage_per_sm = 1;
     int* status = nullptr;
     double* ddiag = nullptr;
     std::vector<void*> state, nl, acc, tw;
@@ -52,6 +62,7 @@ struct ns2d_ensemble {
     cudaGraphExec_t exec = nullptr;
     double graph_dt = -1.0;
     int graph_col_grid = 0, graph_row_grid = 0, graph_col_var = -1, graph_row_var = -1;
+    int graph_fused = -1, graph_stage_grid = 0;
     size_t col_smem[2] = {0, 0}, row_smem[2] = {0, 0};
     int nsm = 148;
 };
@@ -266,6 +277,42 @@ ns2d_status create_t(ns2d_ensemble* e) {
         ECK(e, cudaMemcpyAsync(e->col_items[v], ci.data(), sizeof(EnsItem) * ci.size(), cudaMemcpyHostToDevice, e->stream));
         ECK(e, cudaMemcpyAsync(e->row_items[v], ri.data(), sizeof(EnsItem) * ri.size(), cudaMemcpyHostToDevice, e->stream));
     }
+    {
+        // task list of the per-stage launches, 256-thread shapes
+        std::vector<EnsTask> p1, rows, cols;
+        std::vector<int> need(2 * e->n);
+        for (int m : order) {
+            const int n = e->sizes[m];
+            const int tiles = (n / 2 + 1 + ens_col_tc(n, 0) - 1) / ens_col_tc(n, 0);
+            const int blocks = n / ens_row_tc(n, 0);
+            need[2 * m] = tiles;
+            need[2 * m + 1] = blocks;
+            for (int t = 0; t < tiles; ++t) {
+                p1.push_back({0, m, t});
+                cols.push_back({2, m, t});
+            }
+            for (int r = 0; r < blocks; ++r) rows.push_back({1, m, r});
+        }
+        std::vector<EnsTask> all(p1);
+        all.insert(all.end(), rows.begin(), rows.end());
+        all.insert(all.end(), cols.begin(), cols.end());
+        e->n_tasks = (int)all.size();
+        e->n_p1_tasks = (int)p1.size();
+        ECK(e, alloc(sizeof(EnsTask) * all.size(), (void**)&e->tasks));
+        ECK(e, cudaMemcpyAsync(e->tasks, all.data(), sizeof(EnsTask) * all.size(), cudaMemcpyHostToDevice, e->stream));
+        ECK(e, alloc(sizeof(int) * (4 + 5 * (size_t)e->n), (void**)&e->sync));
+        ECK(e, alloc(sizeof(int) * need.size(), (void**)&e->need));
+        ECK(e, cudaMemcpyAsync(e->need, need.data(), sizeof(int) * need.size(), cudaMemcpyHostToDevice, e->stream));
+        constexpr int TH = kEnsThreadChoices[0];
+        e->stage_smem = EnsSmem<Real, TH>::stage();
+        ECK(e, cudaFuncSetAttribute((const void*)ens_stage_kernel<Real, COL_STAGE, TH>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->stage_smem));
+        ECK(e, cudaFuncSetAttribute((const void*)ens_stage_kernel<Real, COL_FINAL, TH>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->stage_smem));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<Real, COL_STAGE, TH>, TH, e->stage_smem);
+        e->stage_per_sm = std::max(1, per_sm);
+    }
     ECK(e, (ens_set_smem<Real, 0>(e)));
     ECK(e, (ens_set_smem<Real, 1>(e)));
     int dev = 0;
@@ -277,6 +324,7 @@ ns2d_status create_t(ns2d_ensemble* e) {
     e->col_var = e->row_var = 0;
     e->col_grid = std::max(1, std::min(e->n_col_items[0], e->nsm * std::max(1, col_per_sm)));
     e->row_grid = std::max(1, std::min(e->n_row_items[0], e->nsm * std::max(1, row_per_sm)));
+    e->stage_grid = e->nsm * e->stage_per_sm;
     ECK(e, cudaStreamSynchronize(e->stream));
     return NS2D_OK;
 }
@@ -308,6 +356,35 @@ ns2d_status step_t(ns2d_ensemble* e, double dt) {
     st.lin = make_lin_params(e->p, branch);
     st.conj_quirk = (e->p.quirks & NS2D_QUIRK_CONJ_STATE) ? 1 : 0;
     st.status = e->status;
+    if (e->fused) {
+        // one persistent launch per RK stage; the counters restart every step
+        cudaError_t rm = cudaMemsetAsync(e->sync, 0, sizeof(int) * (4 + 5 * (size_t)e->n), e->stream);
+        if (rm != cudaSuccess) return efail(e, NS2D_ERR_CUDA, cudaGetErrorString(rm));
+        EnsSync sy;
+        sy.head = e->sync;
+        sy.done = e->sync + 4;
+        sy.need = e->need;
+        sy.nmem = e->n;
+        constexpr int TH = kEnsThreadChoices[0];
+        for (int s = 1; s <= 4; ++s) {
+            st.stage = s;
+            st.b_cur = explicit_rk4 ? B_ex[s - 1] : B_cn[s - 1];
+            const EnsTask* tl = e->tasks + (s == 1 ? 0 : e->n_p1_tasks);
+            const int nt = e->n_tasks - (s == 1 ? 0 : e->n_p1_tasks);
+            if (s < 4) {
+                st.a_next = A[s - 1];
+                st.first = (s == 1);
+                ens_stage_kernel<Real, COL_STAGE, TH><<<e->stage_grid, TH, e->stage_smem, e->stream>>>(mb, tl, nt, st, sy);
+            } else {
+                st.scheme = explicit_rk4 ? 1 : 0;
+                ens_stage_kernel<Real, COL_FINAL, TH><<<e->stage_grid, TH, e->stage_smem, e->stream>>>(mb, tl, nt, st, sy);
+            }
+            e->launches++;
+        }
+        cudaError_t rf = cudaGetLastError();
+        if (rf != cudaSuccess) return efail(e, NS2D_ERR_CUDA, cudaGetErrorString(rf));
+        return NS2D_OK;
+    }
     st.stage = 0;
     ens_launch_col<Real, COL_P1>(e, mb, st);
     e->launches++;
@@ -338,7 +415,8 @@ ns2d_status step_t(ns2d_ensemble* e, double dt) {
 // branch is settled: capturing records exactly the 9 pass launches.
 ns2d_status ensure_graph(ns2d_ensemble* e, double dt) {
     if (e->exec && e->graph_dt == dt && e->graph_col_grid == e->col_grid && e->graph_row_grid == e->row_grid &&
-        e->graph_col_var == e->col_var && e->graph_row_var == e->row_var)
+        e->graph_col_var == e->col_var && e->graph_row_var == e->row_var && e->graph_fused == (int)e->fused &&
+        e->graph_stage_grid == e->stage_grid)
         return NS2D_OK;
     if (e->exec) {
         cudaGraphExecDestroy(e->exec);
@@ -368,6 +446,8 @@ ns2d_status ensure_graph(ns2d_ensemble* e, double dt) {
     e->graph_row_grid = e->row_grid;
     e->graph_col_var = e->col_var;
     e->graph_row_var = e->row_var;
+    e->graph_fused = (int)e->fused;
+    e->graph_stage_grid = e->stage_grid;
     return NS2D_OK;
 }
 
@@ -392,7 +472,7 @@ ns2d_status step_async_impl(ns2d_ensemble* e, int nsteps, double dt, bool use_gr
         ns2d_status s = ensure_graph(e, dt);
         if (s) return s;
         ECK(e, cudaGraphLaunch(e->exec, e->stream));
-        e->launches += 9;
+        e->launches += e->fused ? 4 : 9;
     }
     return NS2D_OK;
 }
@@ -402,6 +482,7 @@ ns2d_status check_impl(ns2d_ensemble* e) {
     ECK(e, cudaMemcpyAsync(st, e->status, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
     ECK(e, cudaStreamSynchronize(e->stream));
     if (st[0] & 1) return efail(e, NS2D_ERR_BLOWUP, "non-finite vorticity in an ensemble member");
+    if (st[0] & 4) return efail(e, NS2D_ERR_CUDA, "a per-stage launch waited past its bound for a member's tasks");
     return NS2D_OK;
 }
 
@@ -585,7 +666,9 @@ ns2d_status ns2d_ensemble_set_grids(ns2d_ensemble* e, int32_t col_grid, int32_t 
 }
 
 ns2d_status ns2d_ensemble_set_shape(ns2d_ensemble* e, const ns2d_ensemble_shape* sh) {
-    if (!e || !sh || sh->col_grid < 1 || sh->row_grid < 1) return NS2D_ERR_INVALID;
+    if (!e || !sh || sh->col_grid < 1 || sh->row_grid < 1 || sh->stage_launch < 0 || sh->stage_launch > 1 ||
+        (sh->stage_launch && sh->stage_grid < 1))
+        return NS2D_ERR_INVALID;
     int cv = -1, rv = -1;
     for (int v = 0; v < 2; ++v) {
         if (sh->col_threads == kEnsThreadChoices[v]) cv = v;
@@ -596,6 +679,8 @@ ns2d_status ns2d_ensemble_set_shape(ns2d_ensemble* e, const ns2d_ensemble_shape*
     e->row_var = rv;
     e->col_grid = std::min(sh->col_grid, e->n_col_items[cv]);
     e->row_grid = std::min(sh->row_grid, e->n_row_items[rv]);
+    e->fused = sh->stage_launch != 0;
+    if (e->fused) e->stage_grid = std::min(sh->stage_grid, e->n_tasks);
     return NS2D_OK;
 }
 
@@ -605,6 +690,8 @@ ns2d_status ns2d_ensemble_get_shape(const ns2d_ensemble* e, ns2d_ensemble_shape*
     sh->col_grid = e->col_grid;
     sh->row_threads = kEnsThreadChoices[e->row_var];
     sh->row_grid = e->row_grid;
+    sh->stage_launch = e->fused ? 1 : 0;
+    sh->stage_grid = e->stage_grid;
     sh->col_items = e->n_col_items[e->col_var];
     sh->row_items = e->n_row_items[e->row_var];
     return NS2D_OK;
@@ -620,6 +707,7 @@ ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, i
     // SM, capped by the item count), chosen by timing full steps.  Steps taken
     // here advance the members; callers re-set their states.
     const int saved_hyper = e->hyper_flag;
+    e->fused = false;
     EDISPATCH(e, step_t, e, dt);  // settle tables and the operator branch
     cudaStreamSynchronize(e->stream);
     const int mults[] = {1, 2, 3, 4, 6, 8};
@@ -656,6 +744,21 @@ ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, i
             e->row_grid = best_r;
         }
     }
+    // one persistent launch per RK stage, 1..(resident blocks per SM) x SMs
+    bool best_fused = false;
+    int best_sg = e->stage_grid;
+    e->fused = true;
+    for (int k = 1; k <= e->stage_per_sm; ++k) {
+        e->stage_grid = std::min(k * e->nsm, e->n_tasks);
+        const double ms = time_steps(e, dt, 3);
+        if (ms < best) {
+            best = ms;
+            best_fused = true;
+            best_sg = e->stage_grid;
+        }
+    }
+    e->fused = best_fused;
+    e->stage_grid = best_sg;
     e->hyper_flag = saved_hyper;
     cudaError_t r = cudaGetLastError();
     if (r != cudaSuccess) return efail(e, NS2D_ERR_CUDA, cudaGetErrorString(r));

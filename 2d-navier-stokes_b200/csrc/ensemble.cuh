@@ -125,6 +125,110 @@ __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value))
     }
 }
 
+// ---------------------------------------------------------------------------
+// One persistent launch per RK stage.  Launch s (s = 1..4) walks one task list
+// -- the column tiles of the first column pass (s = 1 only), then the row
+// blocks of stage s, then the column tiles of stage s, every member's tasks
+// largest member first -- through a work counter, so tasks are handed out in
+// list order to the blocks that run.  A task of member m waits only for the
+// tasks of m earlier in the same list (its row blocks for the first pass's
+// column tiles, its column tiles for its row blocks): those were handed out
+// before it, to blocks that are running, so every wait ends; members do not
+// wait for each other, and one member's rows overlap another's columns.
+// Each wait is bounded (about 2 s); when a bound is reached the block sets
+// status bit 4 and the launch stops.
+struct EnsTask {
+    int kind;    // 0: first column pass tile, 1: row block, 2: column tile of the stage
+    int member;
+    int tile;
+};
+
+struct EnsSync {
+    int* head;          // [4] work counters of the stage launches
+    int* done;          // [5][nmem]: [0] first-pass column tiles done, [s] row blocks of stage s done
+    const int* need;    // [nmem][2]: column tiles, row blocks of each member
+    int nmem;
+};
+
+__device__ __forceinline__ bool ens_wait_count(const int* cnt, int need, int* status) {
+    long long spins = 0;
+    while (*(volatile const int*)cnt < need) {
+        if (++spins > (1LL << 24)) {
+            atomicOr(status, 4);
+            return false;
+        }
+        __nanosleep(128);
+    }
+    __threadfence();
+    return true;
+}
+
+template <typename Real, int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value))
+    ens_stage_kernel(const EnsMember<Real>* __restrict__ members, const EnsTask* __restrict__ tasks, int ntasks,
+                     EnsStage st, EnsSync sy) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int s_task, s_ok;
+    if (block_should_exit(st.status)) return;
+    for (;;) {
+        if (threadIdx.x == 0) s_task = atomicAdd(sy.head + (st.stage - 1), 1);
+        __syncthreads();
+        const int it = s_task;
+        if (it >= ntasks) return;
+        const EnsTask task = tasks[it];
+        const EnsMember<Real>& mb = members[task.member];
+        // inputs of this task produced earlier in this launch
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (task.kind == 1 && st.stage == 1)
+                ok = ens_wait_count(sy.done + task.member, sy.need[2 * task.member], st.status);
+            else if (task.kind == 2)
+                ok = ens_wait_count(sy.done + (size_t)st.stage * sy.nmem + task.member, sy.need[2 * task.member + 1],
+                                    st.status);
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (task.kind == 1) {
+            switch (mb.n) {
+#define NS2D_ENS_SROW(NN)                                                                 \
+    case NN:                                                                              \
+        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS>(mb.row, task.tile, smraw);       \
+        break;
+                NS2D_ENS_SIZES(NS2D_ENS_SROW)
+#undef NS2D_ENS_SROW
+                default: break;
+            }
+        } else {
+            ColArgs<Real> a = mb.col;
+            EnsStage sc = st;
+            if (task.kind == 0) sc.stage = 0;
+            ens_apply_stage(a, mb, sc);
+            switch (mb.n) {
+#define NS2D_ENS_SCOL(NN)                                                                          \
+    case NN:                                                                                       \
+        if (task.kind == 0) {                                                                      \
+            col_body<Real, NN, EnsShape<NN, THREADS>::TC, COL_P1>(a, task.tile, smraw);            \
+        } else {                                                                                   \
+            col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE>(a, task.tile, smraw);              \
+        }                                                                                          \
+        break;
+                NS2D_ENS_SIZES(NS2D_ENS_SCOL)
+#undef NS2D_ENS_SCOL
+                default: break;
+            }
+        }
+        // this task's outputs are written: every thread fences its stores, then
+        // the task is counted for the tasks that wait on it
+        if (task.kind < 2) {
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(sy.done + (size_t)(task.kind == 0 ? 0 : st.stage) * sy.nmem + task.member, 1);
+        }
+        __syncthreads();
+    }
+}
+
 template <typename Real, int THREADS>
 struct EnsSmem {
     static size_t col() {
@@ -146,6 +250,7 @@ struct EnsSmem {
 #undef NS2D_ENS_RS
         return m;
     }
+    static size_t stage() { return col() > row() ? col() : row(); }
 };
 
 }  // namespace ns2d

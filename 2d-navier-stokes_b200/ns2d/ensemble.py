@@ -13,8 +13,8 @@ _dp = C.POINTER(C.c_double)
 class Shape(C.Structure):
     """struct ns2d_ensemble_shape: block size and persistent grid of the column
     and of the row passes, and (out) the item counts of those shapes."""
-    _fields_ = [(n, C.c_int32) for n in ("col_threads", "col_grid", "row_threads", "row_grid", "col_items",
-                                          "row_items")]
+    _fields_ = [(n, C.c_int32) for n in ("col_threads", "col_grid", "row_threads", "row_grid", "stage_launch",
+                                          "stage_grid", "col_items", "row_items")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -114,8 +114,10 @@ class Ensemble:
         self._ck(self.L.ns2d_ensemble_get_shape(self.h, C.byref(sh)))
         return sh.as_dict()
 
-    def set_shape(self, col_threads, col_grid, row_threads, row_grid):
-        sh = Shape(col_threads=col_threads, col_grid=col_grid, row_threads=row_threads, row_grid=row_grid)
+    def set_shape(self, col_threads=256, col_grid=1184, row_threads=256, row_grid=1184, stage_launch=0,
+                  stage_grid=296):
+        sh = Shape(col_threads=col_threads, col_grid=col_grid, row_threads=row_threads, row_grid=row_grid,
+                   stage_launch=stage_launch, stage_grid=stage_grid)
         self._ck(self.L.ns2d_ensemble_set_shape(self.h, C.byref(sh)))
 
     def set_stream(self, ptr):

@@ -396,21 +396,26 @@ ns2d_status ns2d_ensemble_check(ns2d_ensemble* e);
 ns2d_status ns2d_ensemble_measurables(ns2d_ensemble* e, int32_t member, ns2d_measures* out);
 /* Autotuner: picks, for the column and for the row passes, the block size
    (the tile shape, ns2d_ensemble_shape below) and the persistent grid (1..8
-   blocks per SM) by timing steps at dt; returns the grids.  It advances the
-   members.  ns2d_ensemble_set_grids keeps the block sizes. */
+   blocks per SM), and whether one persistent launch per RK stage beats them,
+   by timing steps at dt; returns the grids of the nine-launch form.  It
+   advances the members.  ns2d_ensemble_set_grids keeps the other choices. */
 ns2d_status ns2d_ensemble_tune(ns2d_ensemble* e, double dt, int32_t* col_grid, int32_t* row_grid);
 ns2d_status ns2d_ensemble_set_grids(ns2d_ensemble* e, int32_t col_grid, int32_t row_grid);
-/* Launch shape of the ensemble's passes: block size of the column and of the
-   row launches (256 or 128 threads; it sets the tile shape -- ky columns per
-   column tile and row pairs per row block of every member, threads / T and
-   threads / 2T with T the threads of one transform of the member's size) and
-   their persistent grids; the item counts of the chosen shapes are reported.
-   ns2d_ensemble_tune picks all four by timing steps (no reference
-   counterpart: the reference runs sweeps as separate processes,
-   Solver/run_solver.py:270-292). */
+/* Launch shape of the ensemble's step.  stage_launch = 0: nine launches, a
+   column and a row pass per stage, with the block size of the column and of
+   the row launches (256 or 128 threads; it sets the tile shape -- ky columns
+   per column tile and row pairs per row block of every member, threads / T
+   and threads / 2T with T the threads of one transform of the member's size)
+   and their persistent grids.  stage_launch = 1: one persistent launch per RK
+   stage (four per step, 256-thread blocks, grid stage_grid) whose tasks wait
+   only for the same member's earlier tasks, so members' passes overlap.  The
+   item counts of the chosen shapes are reported.  ns2d_ensemble_tune picks
+   all of these by timing steps (no reference counterpart: the reference runs
+   sweeps as separate processes, Solver/run_solver.py:270-292). */
 typedef struct ns2d_ensemble_shape {
     int32_t col_threads, col_grid;
     int32_t row_threads, row_grid;
+    int32_t stage_launch, stage_grid;
     int32_t col_items, row_items;   /* out only */
 } ns2d_ensemble_shape;
 ns2d_status ns2d_ensemble_set_shape(ns2d_ensemble* e, const ns2d_ensemble_shape* shape);
