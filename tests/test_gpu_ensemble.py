@@ -122,3 +122,34 @@ def test_block_size_choices_keep_results(col_threads, row_threads):
         assert rel_err(e.get_w_hat(m), ref.get_w_hat(m)) <= 1e-15, m
     e.close()
     ref.close()
+
+
+@pytest.mark.parametrize("precision", [abi.FP64, abi.FP32])
+def test_one_launch_per_stage_equals_nine_launches(precision):
+    """One persistent launch per RK stage (tasks wait only for the same
+    member's earlier tasks) runs the same bodies on the same tiles as the
+    nine-launch step: every member equals it, eagerly and from the captured
+    graph, over several steps -- bit for bit in FP64, within FP32 rounding
+    (1e-5 of max|w_hat|; the two kernels may contract differently) in FP32."""
+    sizes = [512, 64, 256, 128, 128, 512]
+    p = abi.default_params(nu=1e-3, dt=1e-3, precision=precision)
+    ics = _ics(sizes, seed0=120)
+    ref = Ensemble(p, sizes)
+    e = Ensemble(p, sizes)
+    e.set_shape(256, 8 * 148, 256, 8 * 148, stage_launch=1, stage_grid=2 * 148)
+    sh = e.shape
+    assert sh["stage_launch"] == 1 and sh["stage_grid"] >= 1
+    ref.set_shape(256, 8 * 148, 256, 8 * 148, stage_launch=0)
+    for m, w in enumerate(ics):
+        ref.set_w_hat(m, w)
+        e.set_w_hat(m, w)
+    l0 = e.launch_count
+    ref.step_n(7, 1e-3)
+    e.step_n(7, 1e-3)
+    e.check()
+    assert e.launch_count - l0 < 7 * 9  # four launches a step (plus the first steps' tables)
+    tol = 1e-15 if precision == abi.FP64 else 1e-5
+    for m in range(len(sizes)):
+        assert rel_err(e.get_w_hat(m), ref.get_w_hat(m)) <= tol, m
+    e.close()
+    ref.close()
