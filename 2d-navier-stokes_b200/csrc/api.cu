@@ -756,14 +756,27 @@ ns2d_status single_step(ns2d_handle* h, double dt) {
     return DISPATCH(h, rk4_step_impl, h, dt, nullptr);
 }
 
+// Host arrays in the reference layout [nx][ny/2+1] complex128 to and from an
+// internal [nx][ldc] field.  FP64: one strided copy into the padded rows;
+// FP32: through the staging buffer and a converting kernel.
 ns2d_status host_to_state(ns2d_handle* h, const double* host, void* dst) {
+    if (!h->fp32) {
+        CK(h, cudaMemcpy2DAsync(dst, sizeof(double2) * (size_t)h->ldc, host, sizeof(double2) * (size_t)h->nyf,
+                                sizeof(double2) * (size_t)h->nyf, (size_t)h->nx, cudaMemcpyHostToDevice, h->stream));
+        return NS2D_OK;
+    }
     CK(h, cudaMemcpyAsync(h->dio, host, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyHostToDevice, h->stream));
     return DISPATCH(h, pack_in, h, h->dio, dst);
 }
 ns2d_status state_to_host(ns2d_handle* h, const void* src, double* host) {
-    ns2d_status s = DISPATCH(h, unpack_out, h, src, h->dio);
-    if (s) return s;
-    CK(h, cudaMemcpyAsync(host, h->dio, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyDeviceToHost, h->stream));
+    if (!h->fp32) {
+        CK(h, cudaMemcpy2DAsync(host, sizeof(double2) * (size_t)h->nyf, src, sizeof(double2) * (size_t)h->ldc,
+                                sizeof(double2) * (size_t)h->nyf, (size_t)h->nx, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        ns2d_status s = DISPATCH(h, unpack_out, h, src, h->dio);
+        if (s) return s;
+        CK(h, cudaMemcpyAsync(host, h->dio, sizeof(double2) * (size_t)h->nx * h->nyf, cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(h, cudaStreamSynchronize(h->stream));
     return NS2D_OK;
 }
