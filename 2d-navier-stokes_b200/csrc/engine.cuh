@@ -43,6 +43,8 @@ struct Launch {
         set((const void*)col_kernel<Real, N, S::TC, COL_RHS>, col_smem());
         set((const void*)col_kernel<Real, N, S::TC, COL_STAGE>, col_smem());
         set((const void*)col_kernel<Real, N, S::TC, COL_FINAL>, col_smem());
+        set((const void*)col_kernel<Real, N, S::TC, COL_STAGE, true>, col_smem());
+        set((const void*)col_kernel<Real, N, S::TC, COL_FINAL, true>, col_smem());
         set((const void*)row_kernel<Real, N, S::PAIRS>, row_smem());
         set((const void*)col_inv_kernel<Real, N, S::TC>, inv_smem());
         set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, c2r_smem());
@@ -55,11 +57,18 @@ struct Launch {
 
     static void col(int mode, const ColArgs<Real>& a, cudaStream_t s) {
         dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
+        const bool fast = col_fast_ok(a);
         switch (mode) {
             case COL_P1: col_kernel<Real, N, S::TC, COL_P1><<<grid, block, col_smem(), s>>>(a); break;
             case COL_RHS: col_kernel<Real, N, S::TC, COL_RHS><<<grid, block, col_smem(), s>>>(a); break;
-            case COL_STAGE: col_kernel<Real, N, S::TC, COL_STAGE><<<grid, block, col_smem(), s>>>(a); break;
-            default: col_kernel<Real, N, S::TC, COL_FINAL><<<grid, block, col_smem(), s>>>(a); break;
+            case COL_STAGE:
+                if (fast) col_kernel<Real, N, S::TC, COL_STAGE, true><<<grid, block, col_smem(), s>>>(a);
+                else col_kernel<Real, N, S::TC, COL_STAGE><<<grid, block, col_smem(), s>>>(a);
+                break;
+            default:
+                if (fast) col_kernel<Real, N, S::TC, COL_FINAL, true><<<grid, block, col_smem(), s>>>(a);
+                else col_kernel<Real, N, S::TC, COL_FINAL><<<grid, block, col_smem(), s>>>(a);
+                break;
         }
     }
     static void row(const RowArgs<Real>& a, cudaStream_t s) {

@@ -251,7 +251,7 @@ __device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, t
 // threads of a block, thread (t, c) with c = threadIdx.x % TC.  Shared memory:
 // ColSmem::bytes().  Ends with the block synchronised (the shared memory may be
 // reused for another tile).
-template <typename Real, int N, int TC, int MODE>
+template <typename Real, int N, int TC, int MODE, bool FAST = false>
 __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw) {
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
@@ -336,21 +336,25 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             // normalisation and zero mean (solver.c:998-1013)
             C r = (kx == 0 && ky == 0) ? cmake<C>(0, 0) : cscale(sm[q], a.norm2);
             // dealiasing (solver.c:1039-1099)
-            if (a.dealias == 0) {
+            if (FAST || a.dealias == 0) {
                 if ((double)k2 >= (double)a.kmax_sqr || (a.kolm && kx == 0)) r = cmake<C>(0, 0);
             } else {
                 r = cscale(r, houli_filter<Real>(kx, ky, N, N, a.houli_int));
             }
             // forcing (solver.c:1022-1027)
             if (a.has_force && i == a.force_i && ky == a.force_j) r = cadd(r, a.force_val);
-            if (a.force_field) r = cadd(r, a.force_field[(size_t)i * ldc + kyc]);
+            if constexpr (!FAST) {
+                if (a.force_field) r = cadd(r, a.force_field[(size_t)i * ldc + kyc]);
+            }
             if constexpr (MODE == COL_RHS) {
                 // stage derivative with the explicit linear term (Dormand-Prince
                 // stages): r -= bracket(|k|^2) X, X the RHS input
                 if (a.lin_stage == 2 && a.xin && k2 != 0)
                     r = csub(r, cscale(a.xin[(size_t)i * ldc + kyc], (Real)lin_bracket(a.lin, (double)k2)));
             }
-            if (a.rhs_store && valid) a.rhs_store[(size_t)i * ldc + ky] = r;
+            if constexpr (!FAST) {
+                if (a.rhs_store && valid) a.rhs_store[(size_t)i * ldc + ky] = r;
+            }
             // ForceConjugacy side effect on the state (solver.c:1031, 2096-2103)
             C w = cmake<C>(0, 0);
             if constexpr (need_state) w = pre0[q];
@@ -360,7 +364,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             }
             if constexpr (need_state) {
                 // linear term of explicit RK4 stages (solver.c:664-684)
-                if (a.lin_stage && k2 != 0) {
+                if (!FAST && a.lin_stage && k2 != 0) {
                     const C xs = a.xin ? a.xin[(size_t)i * ldc + kyc] : w;
                     const double br = lin_bracket(a.lin, (double)k2);
                     if (a.lin_stage == 1) r = cadd(r, cscale(xs, (Real)(a.dt * br)));
@@ -376,11 +380,13 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                     pre0[q] = nx;
                     if (valid) {
                         if (ky == 0) a.col0_out[i] = nx;
-                        if (a.out) a.out[(size_t)i * ldc + ky] = nx;
+                        if constexpr (!FAST) {
+                            if (a.out) a.out[(size_t)i * ldc + ky] = nx;
+                        }
                     }
                 } else {  // COL_FINAL
                     C tot;
-                    if (a.scheme >= 2) {
+                    if (!FAST && a.scheme >= 2) {
                         // AB4 (solver.c:303-331): 55/24 N_n - 59/24 N_n-1 + 37/24 N_n-2 - 3/8 N_n-3
                         const size_t g = (size_t)i * ldc + kyc;
                         const C p2 = a.h2[g], p1 = a.h1[g], p0 = a.h0[g];
@@ -400,16 +406,16 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                     C wn;
                     if (kx == 0 && ky == 0) {
                         wn = cmake<C>(0, 0);
-                    } else if (a.scheme == 1) {
+                    } else if (!FAST && a.scheme == 1) {
                         wn = cadd(w, cscale(tot, (Real)(a.dt / 6.0)));
-                    } else if (a.scheme == 3) {
+                    } else if (!FAST && a.scheme == 3) {
                         wn = cadd(w, tot);
                     } else {
                         // Crank-Nicolson factors (solver.c:853), from the table
                         const double2 f = a.cn[(size_t)i * ldc + kyc];
                         wn = cadd(cscale(w, (Real)f.x), cscale(tot, (Real)f.y));
                     }
-                    if (a.phase_only && (kx != 0 || ky != 0)) {
+                    if (!FAST && a.phase_only && (kx != 0 || ky != 0)) {
                         // amplitude reset of the phase-only model (solver.c:822-824, 855-857):
                         // w_new *= |w_old| / |w_new|; a mode updated to exactly 0 stays 0
                         const double an = hypot((double)wn.x, (double)wn.y);
@@ -469,11 +475,21 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
 }
 
 // Column pass of one field.  Grid: ceil(nyf / TC) blocks; block: T * TC threads.
-template <typename Real, int N, int TC, int MODE>
+// FAST: the epilogue compiled for the common step only (2/3 dealiasing, no
+// listed-mode forcing, no stored RHS, no explicit linear term, Crank-Nicolson
+// update of the full model); the launcher picks it when the arguments allow.
+template <typename Real, int N, int TC, int MODE, bool FAST = false>
 __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(a.status)) return;
-    col_body<Real, N, TC, MODE>(a, blockIdx.x, smraw);
+    col_body<Real, N, TC, MODE, FAST>(a, blockIdx.x, smraw);
+}
+
+// Whether a stage or final column pass can run the FAST epilogue.
+template <typename Real>
+inline bool col_fast_ok(const ColArgs<Real>& a) {
+    return a.dealias == 0 && !a.force_field && !a.rhs_store && a.lin_stage == 0 && !a.xin && !a.out &&
+           a.scheme == 0 && !a.phase_only;
 }
 
 template <typename Real>
