@@ -125,6 +125,8 @@ cudaError_t ens_set_smem(ns2d_ensemble* e) {
     set((const void*)ens_col_kernel<Real, COL_P1, TH>, e->col_smem[V]);
     set((const void*)ens_col_kernel<Real, COL_STAGE, TH>, e->col_smem[V]);
     set((const void*)ens_col_kernel<Real, COL_FINAL, TH>, e->col_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_STAGE, TH, true>, e->col_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_FINAL, TH, true>, e->col_smem[V]);
     set((const void*)ens_row_kernel<Real, TH>, e->row_smem[V]);
     return r;
 }
@@ -137,15 +139,35 @@ void ens_occupancy(const ns2d_ensemble* e, int* col_per_sm, int* row_per_sm) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(row_per_sm, ens_row_kernel<Real, TH>, TH, e->row_smem[V]);
 }
 
+// Whether the stage and final column passes of this ensemble can run the
+// epilogue compiled for the common step (col_fast_ok of the single passes).
+bool ens_fast(const ns2d_ensemble* e) {
+    return e->p.dealias == 0 && e->p.system != NS2D_EULER && e->p.integrator == NS2D_RK4CN &&
+           e->p.model == NS2D_MODEL_FULL;
+}
+
+template <typename Real, int MODE, int V, bool FAST>
+void ens_launch_col_v(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
+    constexpr int TH = kEnsThreadChoices[V];
+    ens_col_kernel<Real, MODE, TH, FAST><<<e->col_grid, TH, e->col_smem[V], e->stream>>>(mb, e->col_items[V],
+                                                                                       e->n_col_items[V], st);
+}
+
 template <typename Real, int MODE>
 void ens_launch_col(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
-    const int v = e->col_var;
-    if (v == 0)
-        ens_col_kernel<Real, MODE, kEnsThreadChoices[0]><<<e->col_grid, kEnsThreadChoices[0], e->col_smem[0], e->stream>>>(
-            mb, e->col_items[0], e->n_col_items[0], st);
-    else
-        ens_col_kernel<Real, MODE, kEnsThreadChoices[1]><<<e->col_grid, kEnsThreadChoices[1], e->col_smem[1], e->stream>>>(
-            mb, e->col_items[1], e->n_col_items[1], st);
+    if constexpr (MODE == COL_P1) {
+        if (e->col_var == 0) ens_launch_col_v<Real, MODE, 0, false>(e, mb, st);
+        else ens_launch_col_v<Real, MODE, 1, false>(e, mb, st);
+    } else {
+        const bool fast = ens_fast(e);
+        if (e->col_var == 0) {
+            if (fast) ens_launch_col_v<Real, MODE, 0, true>(e, mb, st);
+            else ens_launch_col_v<Real, MODE, 0, false>(e, mb, st);
+        } else {
+            if (fast) ens_launch_col_v<Real, MODE, 1, true>(e, mb, st);
+            else ens_launch_col_v<Real, MODE, 1, false>(e, mb, st);
+        }
+    }
 }
 
 template <typename Real>

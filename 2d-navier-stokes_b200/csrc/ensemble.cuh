@@ -83,7 +83,7 @@ struct EnsMinBlocks {
     static constexpr int value = sizeof(Real) == 4 ? 512 / THREADS : 256 / THREADS;
 };
 
-template <typename Real, int MODE, int THREADS>
+template <typename Real, int MODE, int THREADS, bool FAST = false>
 __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value)) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
                                                       const EnsItem* __restrict__ items, int nitems, EnsStage st) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value))
         switch (mb.n) {
 #define NS2D_ENS_COL(NN)                                                                  \
     case NN:                                                                              \
-        col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE>(a, item.tile, smraw);         \
+        col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE, FAST>(a, item.tile, smraw);   \
         break;
             NS2D_ENS_SIZES(NS2D_ENS_COL)
 #undef NS2D_ENS_COL
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value))
         switch (mb.n) {
 #define NS2D_ENS_ROW(NN)                                                                  \
     case NN:                                                                              \
-        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS>(mb.row, item.tile, smraw);       \
+        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS, false>(mb.row, item.tile, smraw); \
         break;
             NS2D_ENS_SIZES(NS2D_ENS_ROW)
 #undef NS2D_ENS_ROW
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value))
             switch (mb.n) {
 #define NS2D_ENS_SROW(NN)                                                                 \
     case NN:                                                                              \
-        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS>(mb.row, task.tile, smraw);       \
+        row_body<Real, NN, EnsShape<NN, THREADS>::PAIRS, false>(mb.row, task.tile, smraw); \
         break;
                 NS2D_ENS_SIZES(NS2D_ENS_SROW)
 #undef NS2D_ENS_SROW

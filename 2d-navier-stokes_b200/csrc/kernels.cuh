@@ -524,7 +524,7 @@ struct RowSmem {
 // transforms together; rows 2p and 2p+1 then share one packed forward
 // transform, done by team 2p alone when teams are whole warps (team 2p+1
 // leaves) and by both teams, each keeping its half, below a warp.
-template <typename Real, int N, int PAIRS>
+template <typename Real, int N, int PAIRS, bool CAP = true>
 __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, unsigned char* smraw) {
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
@@ -566,7 +566,7 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
         }
     }
     fft_batched<N, +1, 2>(v, pol, seed, t);
-    if (a.cap_uv) {
+    if (CAP && a.cap_uv) {
         C* __restrict__ cu = a.cap_uv + (size_t)x * N;
         C* __restrict__ cw = a.cap_w + (size_t)x * N;
 #pragma unroll
@@ -620,11 +620,13 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
     __syncthreads();  // the shared memory may be reused for another row block
 }
 
-template <typename Real, int N, int PAIRS>
+// CAP: the capture of the real fields (adjoint recomputation) compiled in;
+// the launcher uses the form without it when no capture target is set.
+template <typename Real, int N, int PAIRS, bool CAP = true>
 __global__ void __launch_bounds__(Plan<N>::T * 2 * PAIRS) row_kernel(RowArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(a.status)) return;
-    row_body<Real, N, PAIRS>(a, blockIdx.x, smraw);
+    row_body<Real, N, PAIRS, CAP>(a, blockIdx.x, smraw);
 }
 
 // Crank-Nicolson factors per mode for the current dt and operator branch:
