@@ -2,6 +2,7 @@
 // the host-side sequencing of the step kernels.  Each entry point names the
 // reference function it replaces (EndCar808/2D-Navier-Stokes, Solver/src).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <climits>
@@ -160,10 +161,65 @@ struct TimedLaunch {
     }
 };
 
+// The driver's tensor-map encoder, through the runtime (no libcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor maps for the column passes' TMA tile copies of f[0..3], acc, state and
+// nl (see ColMaps).  Leaves h->col_maps null when a map cannot be encoded; the
+// column passes then copy per thread.
+template <typename Real>
+void build_col_maps(ns2d_handle* h) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    const int tc = col_tc(h->nx);
+    if (!enc || tc == 0) return;
+    auto* m = new (std::nothrow) ColMaps;
+    if (!m) return;
+    const cuuint64_t gdim[2] = {(cuuint64_t)2 * h->nyf, (cuuint64_t)h->nx};
+    const cuuint64_t gstride[1] = {(cuuint64_t)h->ldc * 2 * sizeof(Real)};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)std::min(h->nx, 256)};
+    const cuuint32_t estride[2] = {1, 1};
+    const CUtensorMapDataType dt = sizeof(Real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap* maps[7] = {&m->f[0], &m->f[1], &m->f[2], &m->f[3], &m->acc, &m->state, &m->nl};
+    void* bases[7] = {h->f[0], h->f[1], h->f[2], h->f[3], h->acc, h->state, h->nl};
+    for (int k = 0; k < 7; ++k) {
+        if (enc(maps[k], dt, 2, bases[k], gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+            delete m;
+            return;
+        }
+    }
+    h->col_maps = m;
+}
+
+// The TMA maps when the pass reads and writes exactly the arrays they describe.
+template <typename Real>
+const ColMaps* col_maps_for(const ns2d_handle* h, int mode, const ColArgs<Real>& a) {
+    if (!h->col_maps || mode == COL_RHS) return nullptr;
+    if (mode == COL_P1)
+        return a.src == h->state && a.f0 == h->f[0] && a.f1 == h->f[1] && a.f2 == h->f[2] && a.f3 == h->f[3]
+                   ? static_cast<const ColMaps*>(h->col_maps)
+                   : nullptr;
+    if (a.src != h->nl || a.state != h->state || a.acc != h->acc) return nullptr;
+    if (mode == COL_STAGE && (a.f0 != h->f[0] || a.f1 != h->f[1] || a.f2 != h->f[2] || a.f3 != h->f[3])) return nullptr;
+    return static_cast<const ColMaps*>(h->col_maps);
+}
+
 template <typename Real>
 void launch_col(ns2d_handle* h, int mode, const ColArgs<Real>& a) {
     TimedLaunch t(h, mode == COL_STAGE ? 1 : mode == COL_FINAL ? 2 : 0);
-    with_size<Real>(h->nx, [&](auto L) { decltype(L)::col(mode, a, h->stream); });
+    const ColMaps* maps = col_maps_for<Real>(h, mode, a);
+    with_size<Real>(h->nx, [&](auto L) { decltype(L)::col(mode, a, h->stream, maps); });
 }
 // Row pass of stage `stage` (1..4); with a capture target set, the stage's real
 // fields go to planes 2(stage-1) and 2(stage-1)+1 of it.
@@ -604,6 +660,8 @@ void free_all(ns2d_handle* h) {
     for (void* p : fp)
         if (p) cudaFree(p);
     if (h->dp_kptr) cudaFree((void*)h->dp_kptr);
+    delete static_cast<ColMaps*>(h->col_maps);
+    h->col_maps = nullptr;
 }
 
 template <typename Real>
@@ -633,6 +691,7 @@ ns2d_status create_impl(ns2d_handle* h) {
     CK(h, cudaMalloc(&h->ddiag, sizeof(double) * (DG_N + 8 * (size_t)h->n_spect)));
     CK(h, cudaMalloc(&h->dpart, sizeof(double) * 4096));
     CK(h, cudaMalloc(&h->cn, sizeof(double2) * (size_t)h->nx * h->ldc));
+    build_col_maps<Real>(h);
     CK(h, cudaFuncSetAttribute((const void*)diag_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(sizeof(double) * (8 * (size_t)h->n_spect + DG_N * 8))));
     std::vector<C> tw;
@@ -846,6 +905,7 @@ ns2d_status check_status(ns2d_handle* h) {
     int bits = 0;
     ns2d_status s = read_status(h, &bits, nullptr);
     if (s) return s;
+    if (bits & 8) return fail(h, NS2D_ERR_CUDA, "a column pass waited past its bound for its tile loads");
     if (bits & 1) return fail(h, NS2D_ERR_BLOWUP, "non-finite vorticity (SystemCheck)");
     if (bits & 2) {
         // exact max|w| (GetMaxData("VORT"))

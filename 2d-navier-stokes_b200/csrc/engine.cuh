@@ -25,6 +25,7 @@ struct Launch {
     using S = Shape<N>;
     static constexpr int SIZE = N;
     static constexpr size_t col_smem() { return ColSmem<Real, N, S::TC>::bytes(); }
+    static constexpr size_t col_tma_smem() { return ColSmem<Real, N, S::TC>::bytes() + 1024; }
     static constexpr size_t row_smem() { return RowSmem<Real, N, 2 * S::PAIRS>::bytes(); }
     static constexpr size_t inv_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }
     static constexpr size_t c2r_smem() {
@@ -45,6 +46,9 @@ struct Launch {
         set((const void*)col_kernel<Real, N, S::TC, COL_FINAL>, col_smem());
         set((const void*)col_kernel<Real, N, S::TC, COL_STAGE, true>, col_smem());
         set((const void*)col_kernel<Real, N, S::TC, COL_FINAL, true>, col_smem());
+        set((const void*)col_tma_kernel<Real, N, S::TC, COL_P1>, col_tma_smem());
+        set((const void*)col_tma_kernel<Real, N, S::TC, COL_STAGE>, col_tma_smem());
+        set((const void*)col_tma_kernel<Real, N, S::TC, COL_FINAL>, col_tma_smem());
         set((const void*)row_kernel<Real, N, S::PAIRS>, row_smem());
         set((const void*)col_inv_kernel<Real, N, S::TC>, inv_smem());
         set((const void*)row_c2r_kernel<Real, N, S::PAIRS, R2_MAXABS>, c2r_smem());
@@ -55,18 +59,25 @@ struct Launch {
         return e;
     }
 
-    static void col(int mode, const ColArgs<Real>& a, cudaStream_t s) {
+    // maps: tensor maps of the arrays the pass reads and writes (null: per-thread
+    // copies); the first, stage and final passes then move their tiles by TMA.
+    static void col(int mode, const ColArgs<Real>& a, cudaStream_t s, const ColMaps* maps = nullptr) {
         dim3 grid((a.nyf + S::TC - 1) / S::TC), block(S::T * S::TC);
         const bool fast = col_fast_ok(a);
         switch (mode) {
-            case COL_P1: col_kernel<Real, N, S::TC, COL_P1><<<grid, block, col_smem(), s>>>(a); break;
+            case COL_P1:
+                if (maps) col_tma_kernel<Real, N, S::TC, COL_P1><<<grid, block, col_tma_smem(), s>>>(a, *maps);
+                else col_kernel<Real, N, S::TC, COL_P1><<<grid, block, col_smem(), s>>>(a);
+                break;
             case COL_RHS: col_kernel<Real, N, S::TC, COL_RHS><<<grid, block, col_smem(), s>>>(a); break;
             case COL_STAGE:
-                if (fast) col_kernel<Real, N, S::TC, COL_STAGE, true><<<grid, block, col_smem(), s>>>(a);
+                if (fast && maps) col_tma_kernel<Real, N, S::TC, COL_STAGE><<<grid, block, col_tma_smem(), s>>>(a, *maps);
+                else if (fast) col_kernel<Real, N, S::TC, COL_STAGE, true><<<grid, block, col_smem(), s>>>(a);
                 else col_kernel<Real, N, S::TC, COL_STAGE><<<grid, block, col_smem(), s>>>(a);
                 break;
             default:
-                if (fast) col_kernel<Real, N, S::TC, COL_FINAL, true><<<grid, block, col_smem(), s>>>(a);
+                if (fast && maps) col_tma_kernel<Real, N, S::TC, COL_FINAL><<<grid, block, col_tma_smem(), s>>>(a, *maps);
+                else if (fast) col_kernel<Real, N, S::TC, COL_FINAL, true><<<grid, block, col_smem(), s>>>(a);
                 else col_kernel<Real, N, S::TC, COL_FINAL><<<grid, block, col_smem(), s>>>(a);
                 break;
         }

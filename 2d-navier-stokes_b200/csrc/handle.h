@@ -62,6 +62,7 @@ struct ns2d_handle {
     // adjoint: per-step capture target of the row passes (null = off) and the
     // adjoint's own buffers (adjoint.cu)
     void* cap_step = nullptr;
+    void* col_maps = nullptr;  // ColMaps of f[0..3], acc, state and nl (TMA copies), null if unavailable
     ns2d::AdjointState* adj = nullptr;
     // forcing of listed modes (ns2d_set_forcing_modes): dense field added to the RHS
     void* ffield = nullptr;

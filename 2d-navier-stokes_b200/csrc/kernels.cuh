@@ -20,6 +20,8 @@
 // ldc >= ny/2+1); the intermediate "x-space" arrays use the same shape with
 // the row index meaning x.
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only)
+
 #include "fft.cuh"
 
 namespace ns2d {
@@ -159,6 +161,87 @@ __device__ __forceinline__ void cp_async_elem(C* smem, const C* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Tensor maps of the arrays a column pass moves by TMA tile copies: the four
+// x-space fields, the RK accumulator, the state and the product spectrum (the
+// stage and final passes' input), each a 2-D array of nx rows by 2*nyf reals
+// (row stride ldc complex) with boxes of (2*TC reals, min(nx, 256) rows), i.e.
+// one column tile in the [row][TC] order of the staging buffers.  Columns at or
+// past nyf lie outside the maps: loads read zeros there and stores clip them.
+struct ColMaps {
+    CUtensorMap f[4];
+    CUtensorMap acc;
+    CUtensorMap state;
+    CUtensorMap nl;
+};
+
+// Bulk-async (TMA) tile stores, shared memory -> global.  The staging writes of
+// every thread are made visible to the async proxy (fence) and joined by a
+// barrier before one thread issues the copies.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the shared-memory sources of all committed stores have been read
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// all committed stores have completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// mbarrier helpers for the TMA tile loads (one barrier per group of loads,
+// used once per block: phase 0).
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// Bounded wait for phase 0 of `bar`: false if the loads have not landed after
+// 2^22 polls (each poll may suspend the thread for a while in hardware).
+__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar) {
+    const unsigned a = smem_addr(bar);
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Load column tile `tile` through `map` into dst ([N][TC] complex, dense),
+// completing on `bar` (whose expected byte count covers it).
+template <typename C, int N, int TC>
+__device__ __forceinline__ void tma_load_tile(const CUtensorMap* map, int tile, C* dst, unsigned long long* bar) {
+    constexpr int BR = N < 256 ? N : 256;
+    static_assert(((TC * sizeof(C)) % 16) == 0, "TMA x extent must be a multiple of 16 bytes");
+    const int x = tile * TC * 2;  // in reals: a multiple of 16 bytes
+#pragma unroll
+    for (int q = 0; q < N / BR; ++q) {
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+                smem_addr(dst + (size_t)q * BR * TC)),
+            "l"(map), "r"(x), "r"(q * BR), "r"(smem_addr(bar))
+            : "memory");
+    }
+}
+
+// Store column tile `tile` ([N][TC] complex, dense, at stg) through `map`.
+template <typename C, int N, int TC>
+__device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, int tile, const C* stg) {
+    constexpr int BR = N < 256 ? N : 256;
+    static_assert(((TC * sizeof(C)) % 16) == 0, "TMA x extent must be a multiple of 16 bytes");
+    const int x = tile * TC * 2;  // in reals: a multiple of 16 bytes
+#pragma unroll
+    for (int q = 0; q < N / BR; ++q) {
+        const unsigned src = (unsigned)__cvta_generic_to_shared(stg + (size_t)q * BR * TC);
+        asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(map),
+                     "r"(x), "r"(q * BR), "r"(src)
+                     : "memory");
+    }
+}
+
 // Shared memory of the column pass: two FFT exchange buffers (the second one
 // first holds the prefetched RK accumulator), then the [N][TC] staging array
 // of the state, which becomes the next stage input X.
@@ -171,30 +254,43 @@ struct ColSmem {
     static constexpr size_t bytes() { return sizeof(C) * (size_t)(2 * FFT + PRE); }
 };
 
-// 1/k^2 for the velocity spectra.  FP64: Newton-Raphson for the reciprocal,
-// r <- r + r (1 - k2 r), twice from the single-precision reciprocal (k2 < 2^24
-// is exact in FP32, the seed's relative error is below 2^-23, so two steps
-// leave about one rounding of FP64); single precision in the FP32 form.
+// 1/k^2 for the velocity spectra, k2 = kx^2 + ky^2 >= 1 held exactly.  FP64:
+// Newton-Raphson for the reciprocal, r <- r + r (1 - k2 r), twice from the
+// hardware approximation (PTX rcp.approx.ftz.f64, relative error far below
+// 2^-14, so two quadratic steps leave about one rounding of FP64); the FP32
+// form is the correctly rounded single-precision reciprocal.
 template <typename Real>
-__device__ __forceinline__ Real inv_k2(int k2);
+__device__ __forceinline__ Real inv_k2(Real k2);
 template <>
-__device__ __forceinline__ double inv_k2<double>(int k2) {
-    const double d = (double)k2;
-    double r = (double)__frcp_rn((float)k2);
-    r = fma(r, fma(-d, r, 1.0), r);
-    r = fma(r, fma(-d, r, 1.0), r);
+__device__ __forceinline__ double inv_k2<double>(double k2) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(k2));
+    r = fma(r, fma(-k2, r, 1.0), r);
+    r = fma(r, fma(-k2, r, 1.0), r);
     return r;
 }
 template <>
-__device__ __forceinline__ float inv_k2<float>(int k2) { return __frcp_rn((float)k2); }
+__device__ __forceinline__ float inv_k2<float>(float k2) { return __frcp_rn(k2); }
+
+// kx of transform element m (row i = t + T m of an N-row column) as a real:
+// i for i <= N/2, i - N above; tr = (Real)t.  m is a compile-time index in the
+// unrolled loops, so only the element that can hold i = N/2 needs a select.
+template <typename Real, int N, int T>
+__device__ __forceinline__ Real kx_of(int m, int t, Real tr) {
+    constexpr int H = N / (2 * T);
+    if (m < H) return tr + (Real)(T * m);
+    if (m > H) return tr + (Real)(T * m - N);
+    return t == 0 ? (Real)(N / 2) : tr + (Real)(T * m - N);
+}
 
 // Derived spectra of the stage input X at (kx, ky) (solver.c:904-957), two at a
 // time: pair 0 gives u = i ky/k^2 X and v = -i kx/k^2 X (one reciprocal), pair 2
-// gives w_x = i kx X and w_y = i ky X.  Zero at the mean mode.
+// gives w_x = i kx X and w_y = i ky X.  Zero at the mean mode.  kx and ky are
+// integers held as reals.
 template <typename C>
-__device__ __forceinline__ void derived_pair(int fp, int kx, int ky, C X, C& a, C& b) {
+__device__ __forceinline__ void derived_pair(int fp, decltype(C::x) kx, decltype(C::x) ky, C X, C& a, C& b) {
     using Real = decltype(C::x);
-    if (kx == 0 && ky == 0) {
+    if (kx == (Real)0 && ky == (Real)0) {
         a = cmake<C>(0, 0);
         b = a;
         return;
@@ -202,11 +298,11 @@ __device__ __forceinline__ void derived_pair(int fp, int kx, int ky, C X, C& a, 
     Real sa, sb;
     if (fp == 0) {
         const Real inv = inv_k2<Real>(kx * kx + ky * ky);
-        sa = (Real)ky * inv;
-        sb = -(Real)kx * inv;
+        sa = ky * inv;
+        sb = -kx * inv;
     } else {
-        sa = (Real)kx;
-        sb = (Real)ky;
+        sa = kx;
+        sb = ky;
     }
     // i s X = (-s X.y, s X.x)
     a = cmake<C>(-sa * X.y, sa * X.x);
@@ -225,14 +321,14 @@ __device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, t
     constexpr int T = Plan<N>::T;
     constexpr int E = N / T;
     C* outs[4] = {f0, f1, f2, f3};
+    const Real tr = (Real)t, kyr = (Real)ky;
 #pragma unroll 1
     for (int fp = 0; fp < 4; fp += 2) {
         C v[2][E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
-            const int kx = (i <= N / 2) ? i : i - N;
-            derived_pair(fp, kx, ky, pre0[i * TC + c], v[0][m], v[1][m]);
+            derived_pair(fp, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
         }
         fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
         if (valid) {
@@ -247,12 +343,65 @@ __device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, t
     }
 }
 
+// derived_ifft with TMA stores: each pair's outputs are staged densely in the
+// two exchange buffers (free once the pair's transform has passed its last
+// barrier) and stored by one thread as bulk-async tile copies, so the warps go
+// on to the next pair while the copy engine drains the stores.  pending: a
+// store issued before this call still reads the exchange buffers (the
+// accumulator, staged in the second one).  Thread 0 returns once all stores
+// have completed.
+template <typename Real, int N, int TC>
+__device__ __forceinline__ void derived_ifft_tma(const typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
+                                                 const ColMaps* maps, int tile, int ky, int t, int c,
+                                                 TwSeed<typename Cx<Real>::T> seed, bool pending) {
+    using C = typename Cx<Real>::T;
+    constexpr int T = Plan<N>::T;
+    constexpr int E = N / T;
+    constexpr int STRIDE = SmemLayout<N, TC>::ELEMS;
+    const Real tr = (Real)t, kyr = (Real)ky;
+#pragma unroll 1
+    for (int fp = 0; fp < 4; fp += 2) {
+        C v[2][E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int i = t + T * m;
+            derived_pair(fp, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
+        }
+        if (pending || fp > 0) {
+            if (threadIdx.x == 0) bulk_wait_read_all();
+            __syncthreads();
+        }
+        fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            sm[(t + T * m) * TC + c] = v[0][m];
+            sm[STRIDE + (t + T * m) * TC + c] = v[1][m];
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tma_store_tile<C, N, TC>(&maps->f[fp], tile, sm);
+            tma_store_tile<C, N, TC>(&maps->f[fp + 1], tile, sm + STRIDE);
+            bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) bulk_wait_all();
+}
+
 // Column pass on tile `tile` (ky columns tile*TC .. tile*TC+TC-1), by the T*TC
 // threads of a block, thread (t, c) with c = threadIdx.x % TC.  Shared memory:
 // ColSmem::bytes().  Ends with the block synchronised (the shared memory may be
 // reused for another tile).
-template <typename Real, int N, int TC, int MODE, bool FAST = false>
-__device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw) {
+// TMA (with FAST, modes P1, STAGE and FINAL): the pass's inputs (a.src, a.state,
+// a.acc) arrive by TMA tile loads and its outputs (the x-space fields, the
+// accumulator, the final state) leave by bulk-async tile stores, through `maps`
+// (which must describe those arrays), instead of per-thread copies; smraw
+// 1024-byte aligned.  A load that does not land within its bound sets status
+// bit 8 and the block returns.
+template <typename Real, int N, int TC, int MODE, bool FAST = false, bool TMA = false>
+__device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw,
+                                         const ColMaps* maps = nullptr) {
+    static_assert(!TMA || (FAST && MODE != COL_RHS), "TMA copies: FAST P1, STAGE and FINAL only");
     using C = typename Cx<Real>::T;
     using P = Plan<N>;
     using SM = ColSmem<Real, N, TC>;
@@ -270,15 +419,33 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
     const TwSeed<C> seed = twiddle_seeds<N>(a.tw, t);
 
     if constexpr (MODE == COL_P1) {
-        const C* __restrict__ src = a.src;
+        if constexpr (TMA) {
+            __shared__ __align__(8) unsigned long long bar_in;
+            if (threadIdx.x == 0) {
+                mbar_init(&bar_in);
+                mbar_expect_tx(&bar_in, (unsigned)(sizeof(C) * N * TC));
+                tma_load_tile<C, N, TC>(&maps->state, tile, pre0, &bar_in);
+            }
+            __syncthreads();
+            const bool late = !mbar_wait0(&bar_in);
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) {
+                    atomicOr(a.status, 8);
+                    mbar_wait0(&bar_in);
+                }
+                return;
+            }
+        } else {
+            const C* __restrict__ src = a.src;
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int i = t + T * m;
-            if (valid) cp_async_elem(pre0 + i * TC + c, src + (size_t)i * ldc + ky);
-            else pre0[i * TC + c] = cmake<C>(0, 0);
+            for (int m = 0; m < E; ++m) {
+                const int i = t + T * m;
+                if (valid) cp_async_elem(pre0 + i * TC + c, src + (size_t)i * ldc + ky);
+                else pre0[i * TC + c] = cmake<C>(0, 0);
+            }
+            cp_async_commit();
+            cp_async_wait_all();
         }
-        cp_async_commit();
-        cp_async_wait_all();
         if (a.col0_out && ky == 0) {
             // snapshot of the input's column 0 for a later conjugacy step whose
             // kernel also rewrites the state (AB4 update)
@@ -288,15 +455,41 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
     } else {
         const C* __restrict__ src = a.src;
         C v[1][E];
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int i = t + T * m;
-            v[0][m] = valid ? src[(size_t)i * ldc + kyc] : cmake<C>(0, 0);
-        }
-        // prefetch the epilogue operands while the forward transform runs
         constexpr bool need_state = (MODE == COL_STAGE || MODE == COL_FINAL);
         const bool need_acc = (MODE == COL_STAGE && !a.first) || (MODE == COL_FINAL && a.scheme < 2);
-        if constexpr (need_state) {
+        __shared__ __align__(8) unsigned long long bar_tile[2];  // TMA: [0] the input, [1] state and accumulator
+        if constexpr (TMA) {
+            if (threadIdx.x == 0) {
+                mbar_init(&bar_tile[0]);
+                mbar_init(&bar_tile[1]);
+                constexpr unsigned tile_bytes = (unsigned)(sizeof(C) * N * TC);
+                mbar_expect_tx(&bar_tile[0], tile_bytes);
+                tma_load_tile<C, N, TC>(&maps->nl, tile, sm, &bar_tile[0]);
+                mbar_expect_tx(&bar_tile[1], need_acc ? 2 * tile_bytes : tile_bytes);
+                tma_load_tile<C, N, TC>(&maps->state, tile, pre0, &bar_tile[1]);
+                if (need_acc) tma_load_tile<C, N, TC>(&maps->acc, tile, pre1, &bar_tile[1]);
+            }
+            __syncthreads();
+            const bool late = !mbar_wait0(&bar_tile[0]);
+#pragma unroll
+            for (int m = 0; m < E; ++m) v[0][m] = sm[(t + T * m) * TC + c];
+            // every thread has its input before the transform reuses the buffer
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) {
+                    atomicOr(a.status, 8);
+                    mbar_wait0(&bar_tile[1]);
+                }
+                return;
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int i = t + T * m;
+                v[0][m] = valid ? src[(size_t)i * ldc + kyc] : cmake<C>(0, 0);
+            }
+        }
+        // prefetch the epilogue operands while the forward transform runs
+        if constexpr (need_state && !TMA) {
 #pragma unroll
             for (int m = 0; m < E; ++m) {
                 const int i = t + T * m;
@@ -324,10 +517,20 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
         // buffer, in slots only this thread touches.
 #pragma unroll
         for (int m = 0; m < E; ++m) sm[(t + T * m) * TC + c] = v[0][m];
-        if constexpr (need_state) cp_async_wait_all();
+        if constexpr (TMA) {
+            const bool late = !mbar_wait0(&bar_tile[1]);
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) atomicOr(a.status, 8);
+                return;
+            }
+        } else if constexpr (need_state) {
+            cp_async_wait_all();
+        }
         double bsum = 0.0;
         bool bad = false;
-#pragma unroll 4
+        // FAST: fully unrolled (its epilogue is short enough); else four at a time
+        constexpr int EU = FAST ? E : 4;
+#pragma unroll EU
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
             const int q = i * TC + c;
@@ -337,7 +540,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             C r = (kx == 0 && ky == 0) ? cmake<C>(0, 0) : cscale(sm[q], a.norm2);
             // dealiasing (solver.c:1039-1099)
             if (FAST || a.dealias == 0) {
-                if ((double)k2 >= (double)a.kmax_sqr || (a.kolm && kx == 0)) r = cmake<C>(0, 0);
+                if (k2 >= a.kmax_sqr || (a.kolm && kx == 0)) r = cmake<C>(0, 0);
             } else {
                 r = cscale(r, houli_filter<Real>(kx, ky, N, N, a.houli_int));
             }
@@ -360,7 +563,8 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             if constexpr (need_state) w = pre0[q];
             if (a.conj_mode && ky == 0 && kx < 0 && valid) {
                 w = cconj(a.conj_src[(size_t)(-kx) * a.conj_stride]);
-                a.state[(size_t)i * ldc] = w;
+                // (the TMA final pass stores this element's update through the tile copy)
+                if constexpr (!(TMA && MODE == COL_FINAL)) a.state[(size_t)i * ldc] = w;
             }
             if constexpr (need_state) {
                 // linear term of explicit RK4 stages (solver.c:664-684)
@@ -374,7 +578,8 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                     C acc;
                     if (a.first) acc = cscale(r, (Real)a.b_cur);
                     else acc = cadd(pre1[q], cscale(r, (Real)a.b_cur));
-                    if (valid) a.acc[(size_t)i * ldc + ky] = acc;
+                    if constexpr (TMA) pre1[q] = acc;  // staged for the tile store
+                    else if (valid) a.acc[(size_t)i * ldc + ky] = acc;
                     const Real adt = (Real)(a.dt * a.a_next);
                     const C nx = cadd(w, cscale(r, adt));
                     pre0[q] = nx;
@@ -424,8 +629,9 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                             wn = cmake<C>((Real)((double)wn.x * r), (Real)((double)wn.y * r));
                         }
                     }
+                    if constexpr (TMA) pre0[q] = wn;  // staged for the tile store
                     if (valid) {
-                        a.state[(size_t)i * ldc + ky] = wn;
+                        if constexpr (!TMA) a.state[(size_t)i * ldc + ky] = wn;
                         const double mag = fabs((double)wn.x) + fabs((double)wn.y);
                         bad |= !isfinite(mag);
                         bsum += (ky == 0 || 2 * ky == N) ? mag : 2.0 * mag;
@@ -434,12 +640,28 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             }
         }
         // the next transform's first stage writes other threads' parked slots
+        if constexpr (TMA) fence_async_smem();
         __syncthreads();
+        if constexpr (TMA && MODE == COL_STAGE) {
+            if (threadIdx.x == 0) {
+                tma_store_tile<C, N, TC>(&maps->acc, tile, pre1);
+                bulk_commit();
+            }
+        }
+        if constexpr (TMA && MODE == COL_FINAL) {
+            if (threadIdx.x == 0) {
+                tma_store_tile<C, N, TC>(&maps->state, tile, pre0);
+                bulk_commit();
+            }
+        }
         if constexpr (MODE == COL_FINAL) {
             if (!a.final_tail) {
                 // ensemble form: only the non-finite check
                 if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(a.status, 1);
                 __syncthreads();
+                if constexpr (TMA) {
+                    if (threadIdx.x == 0) bulk_wait_all();
+                }
                 return;
             }
             // SystemCheck (solver.c:2301-2326) without a transform: max|w(x)| is
@@ -466,12 +688,16 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 if (tile == 0) atomicAdd(a.status + 1, 1);  // completed steps
             }
             __syncthreads();
+            if constexpr (TMA) {
+                if (threadIdx.x == 0) bulk_wait_all();
+            }
             return;
         }
         if constexpr (MODE == COL_RHS) return;
     }
 
-    derived_ifft<Real, N, TC>(pre0, sm, a.f0, a.f1, a.f2, a.f3, ldc, ky, valid, t, c, seed);
+    if constexpr (TMA) derived_ifft_tma<Real, N, TC>(pre0, sm, maps, tile, ky, t, c, seed, MODE == COL_STAGE);
+    else derived_ifft<Real, N, TC>(pre0, sm, a.f0, a.f1, a.f2, a.f3, ldc, ky, valid, t, c, seed);
 }
 
 // Column pass of one field.  Grid: ceil(nyf / TC) blocks; block: T * TC threads.
@@ -483,6 +709,16 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(a.status)) return;
     col_body<Real, N, TC, MODE, FAST>(a, blockIdx.x, smraw);
+}
+
+// Column pass with TMA tile loads and stores (FAST P1, STAGE and FINAL).  Shared
+// memory: ColSmem::bytes() + 1024 (the body's base is rounded up to 1024 bytes).
+template <typename Real, int N, int TC, int MODE>
+__global__ void __launch_bounds__(Plan<N>::T * TC) col_tma_kernel(ColArgs<Real> a, const __grid_constant__ ColMaps maps) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    if (block_should_exit(a.status)) return;
+    unsigned char* sm = smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
+    col_body<Real, N, TC, MODE, true, true>(a, blockIdx.x, sm, &maps);
 }
 
 // Whether a stage or final column pass can run the FAST epilogue.
