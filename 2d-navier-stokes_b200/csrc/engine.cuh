@@ -25,7 +25,7 @@ struct Launch {
     using S = Shape<N>;
     static constexpr int SIZE = N;
     static constexpr size_t col_smem() { return ColSmem<Real, N, S::TC>::bytes(); }
-    static constexpr size_t col_tma_smem() { return ColSmem<Real, N, S::TC>::bytes() + 1024; }
+    static constexpr size_t col_tma_smem() { return ColSmem<Real, N, S::TC>::bytes_tma() + 1024; }
     static constexpr size_t row_smem() { return RowSmem<Real, N, 2 * S::PAIRS>::bytes(); }
     static constexpr size_t inv_smem() { return sizeof(C) * SmemLayout<N, S::TC>::ELEMS; }
     static constexpr size_t c2r_smem() {

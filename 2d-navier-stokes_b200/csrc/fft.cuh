@@ -277,6 +277,16 @@ struct IlvPolicy {
     __device__ __forceinline__ C& at(int b, int e) const { return sm[b * STRIDE + SmemLayout<N, TC>::slot(e, c)]; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
+// Interleaved over two buffers at arbitrary places (p0 for batch entry 0, p1
+// for entry 1), synchronised with the block barrier.
+template <int N, int TC, typename C>
+struct IlvPairPolicy {
+    C* p0;
+    C* p1;
+    int c;
+    __device__ __forceinline__ C& at(int b, int e) const { return (b ? p1 : p0)[SmemLayout<N, TC>::slot(e, c)]; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
 // Team: private padded regions, named barrier (or warp barrier below 32 threads).
 template <int N, typename C>
 struct TeamPolicy {

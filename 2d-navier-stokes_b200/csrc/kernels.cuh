@@ -252,6 +252,9 @@ struct ColSmem {
     static constexpr int PRE = N * TC;
     static_assert(FFT >= PRE, "accumulator staging must fit the second exchange buffer");
     static constexpr size_t bytes() { return sizeof(C) * (size_t)(2 * FFT + PRE); }
+    // the TMA form: the third region is a full exchange buffer too (the second
+    // inverse pair transforms in it while the first pair's stores drain)
+    static constexpr size_t bytes_tma() { return sizeof(C) * (size_t)(3 * FFT); }
 };
 
 // 1/k^2 for the velocity spectra, k2 = kx^2 + ky^2 >= 1 held exactly.  FP64:
@@ -343,15 +346,16 @@ __device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, t
     }
 }
 
-// derived_ifft with TMA stores: each pair's outputs are staged densely in the
-// two exchange buffers (free once the pair's transform has passed its last
-// barrier) and stored by one thread as bulk-async tile copies, so the warps go
-// on to the next pair while the copy engine drains the stores.  pending: a
-// store issued before this call still reads the exchange buffers (the
-// accumulator, staged in the second one).  Thread 0 returns once all stores
-// have completed.
+// derived_ifft with TMA stores.  The three shared regions B0 = sm, B1 = sm +
+// STRIDE and B2 = pre0 (sized as an exchange buffer in this form) rotate: the
+// first pair transforms in (B0, B1) and is staged there, each field stored by
+// its own bulk-async group; the second pair's spectra are formed from B2 (the
+// stage input), which is then free, so it transforms in (B2, B0) as soon as
+// the first field's store has read B0, while the second field still drains
+// from B1.  pending: a store issued before this call still reads B1 (the
+// accumulator).  Thread 0 returns once all stores have completed.
 template <typename Real, int N, int TC>
-__device__ __forceinline__ void derived_ifft_tma(const typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
+__device__ __forceinline__ void derived_ifft_tma(typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
                                                  const ColMaps* maps, int tile, int ky, int t, int c,
                                                  TwSeed<typename Cx<Real>::T> seed, bool pending) {
     using C = typename Cx<Real>::T;
@@ -359,6 +363,9 @@ __device__ __forceinline__ void derived_ifft_tma(const typename Cx<Real>::T* pre
     constexpr int E = N / T;
     constexpr int STRIDE = SmemLayout<N, TC>::ELEMS;
     const Real tr = (Real)t, kyr = (Real)ky;
+    C* const B0 = sm;
+    C* const B1 = sm + STRIDE;
+    C* const B2 = pre0;
 #pragma unroll 1
     for (int fp = 0; fp < 4; fp += 2) {
         C v[2][E];
@@ -367,21 +374,30 @@ __device__ __forceinline__ void derived_ifft_tma(const typename Cx<Real>::T* pre
             const int i = t + T * m;
             derived_pair(fp, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
         }
-        if (pending || fp > 0) {
-            if (threadIdx.x == 0) bulk_wait_read_all();
+        // first pair: the accumulator store (if any) must have read B1;
+        // second pair: the first pair's first field must have left B0 (at
+        // most its second group still pending), and every thread has read B2
+        if (fp == 0 ? pending : true) {
+            if (threadIdx.x == 0) {
+                if (fp == 0) bulk_wait_read_all();
+                else asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+            }
             __syncthreads();
         }
-        fft_batched<N, +1, 2>(v, IlvPolicy<N, TC, C>{sm, c}, seed, t);
+        C* const Pa = fp == 0 ? B0 : B2;
+        C* const Pb = fp == 0 ? B1 : B0;
+        fft_batched<N, +1, 2>(v, IlvPairPolicy<N, TC, C>{Pa, Pb, c}, seed, t);
 #pragma unroll
         for (int m = 0; m < E; ++m) {
-            sm[(t + T * m) * TC + c] = v[0][m];
-            sm[STRIDE + (t + T * m) * TC + c] = v[1][m];
+            Pa[(t + T * m) * TC + c] = v[0][m];
+            Pb[(t + T * m) * TC + c] = v[1][m];
         }
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
-            tma_store_tile<C, N, TC>(&maps->f[fp], tile, sm);
-            tma_store_tile<C, N, TC>(&maps->f[fp + 1], tile, sm + STRIDE);
+            tma_store_tile<C, N, TC>(&maps->f[fp], tile, Pa);
+            bulk_commit();
+            tma_store_tile<C, N, TC>(&maps->f[fp + 1], tile, Pb);
             bulk_commit();
         }
     }
@@ -712,7 +728,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_kernel(ColArgs<Real> a) {
 }
 
 // Column pass with TMA tile loads and stores (FAST P1, STAGE and FINAL).  Shared
-// memory: ColSmem::bytes() + 1024 (the body's base is rounded up to 1024 bytes).
+// memory: ColSmem::bytes_tma() + 1024 (the body's base is rounded up to 1024 bytes).
 template <typename Real, int N, int TC, int MODE>
 __global__ void __launch_bounds__(Plan<N>::T * TC) col_tma_kernel(ColArgs<Real> a, const __grid_constant__ ColMaps maps) {
     extern __shared__ __align__(16) unsigned char smraw[];
