@@ -167,6 +167,18 @@ __device__ __forceinline__ TwSeed<C> twiddle_seeds(const C* __restrict__ tw, int
     return s;
 }
 
+// Seeds of the N-point plan read from the table of a multiple of N points:
+// tw[stride * j] = exp(-2 pi i j / N).
+template <int N, typename C>
+__device__ __forceinline__ TwSeed<C> twiddle_seeds_strided(const C* __restrict__ tw, int t, int stride) {
+    using P = Plan<N>;
+    TwSeed<C> s;
+    constexpr int NS1 = P::R0;
+    s.mid = __ldg(tw + stride * ((t % NS1) * (N / (NS1 * P::R1))));
+    s.last = __ldg(tw + stride * t);
+    return s;
+}
+
 // out[r] = w^r for r < R (out[0] unused), with conj(w) for SIGN > 0.
 template <int R, int SIGN, typename C>
 __device__ __forceinline__ void tw_powers(C w, C* out) {

@@ -771,6 +771,13 @@ struct RowSmem {
     static constexpr size_t bytes() { return sizeof(C) * (size_t)TEAM * TC; }
 };
 
+// Team width of the N/2-point plan (0 below the smallest plan).
+template <int N>
+constexpr int half_plan_width() {
+    if constexpr (N / 2 >= 16) return Plan<N / 2>::T;
+    else return 0;
+}
+
 // Row pass.  Block: TC = 2*PAIRS rows, one team of T threads per row (whole
 // warps when T >= 32); grid: nrows / TC.  Each team runs its row's two inverse
 // transforms together; rows 2p and 2p+1 then share one packed forward
@@ -831,6 +838,40 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
     Real* nl_own = reinterpret_cast<Real*>(region + TL::ROWS);
 #pragma unroll
     for (int m = 0; m < E; ++m) nl_own[t + T * m] = v[0][m].x * v[1][m].x + v[0][m].y * v[1][m].y;
+    // HALF: each team transforms its own row's real product as an N/2-point
+    // complex sequence z[j] = n[2j] + i n[2j+1] and splits the result,
+    //   X[k] = (Z[k] + conj Z[N/2-k])/2 + W^k (Z[k] - conj Z[N/2-k])/(2i),
+    // W = exp(-2 pi i / N), k = 0..N/2 (Z periodic in N/2): both teams work and
+    // only team barriers are needed.  Where the N/2 plan has another team width
+    // the rows of a pair share one packed N-point transform instead.
+    constexpr int NH = N / 2;
+    constexpr bool HALF = (T >= 32) && (half_plan_width<N>() == T);
+    if constexpr (HALF) {
+        constexpr int EH = NH / T;
+        using TLH = TeamLayout<NH>;
+        static_assert(TLH::ROWS <= TL::ROWS, "the half-size exchange must not reach the parked product");
+        pol.sync();
+        const C* zin = reinterpret_cast<const C*>(nl_own);
+        C z[1][EH];
+#pragma unroll
+        for (int m = 0; m < EH; ++m) z[0][m] = zin[t + T * m];
+        const TeamPolicy<NH, C> polh{region, 1 + g};
+        fft_batched<NH, -1, 1>(z, polh, twiddle_seeds_strided<NH>(a.tw, t, 2), t);
+#pragma unroll
+        for (int m = 0; m < EH; ++m) region[TLH::slot(t + T * m)] = z[0][m];
+        polh.sync();
+        C* dst = a.nl + (size_t)x * a.ldc;
+#pragma unroll
+        for (int m = 0; m < EH; ++m) {
+            const int k = t + T * m;
+            const C zk = z[0][m];
+            const C zm = region[TLH::slot((NH - k) & (NH - 1))];
+            const C ev = cmake<C>((Real)0.5 * (zk.x + zm.x), (Real)0.5 * (zk.y - zm.y));
+            const C od = cmake<C>((Real)0.5 * (zk.y + zm.y), (Real)0.5 * (zm.x - zk.x));
+            dst[k] = cadd(ev, cmul(__ldg(a.tw + k), od));
+            if (k == 0) dst[NH] = cmake<C>(zk.x - zk.y, (Real)0);  // W^(N/2) = -1
+        }
+    } else {
     __syncthreads();
     const int ga = g & ~1;
     bool active = true;
@@ -869,6 +910,7 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
         }
     }
     }  // active
+    }  // HALF
     __syncthreads();  // the shared memory may be reused for another row block
 }
 
