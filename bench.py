@@ -381,8 +381,11 @@ def adjoint_bench(stream, nsteps, rank, precision, g_ref=None, n_dirs=16):
     50 steps): device time of one gradient of the final enstrophy (record +
     objective + checkpointed reverse sweep) over the time of the forward solve
     alone, from w0 = decaying spectrum (k0 = 4) projected to E = 0.5, Z = 10.
-    FP64: central differences (eps = 1e-6, |d|_W = |w0|_W) of the forward along
-    n_dirs seeded directions.  FP32: the gradient against the FP64 one (g_ref)."""
+    FP64: central differences (eps in 1e-5, 1e-6, 1e-7, |d|_W = |w0|_W) of the
+    forward along n_dirs seeded directions; the headline `fd` figures are those
+    of the one eps whose worst direction agrees best (the same eps for every
+    direction), the whole sweep is reported beside them.  FP32: the gradient
+    against the FP64 one (g_ref)."""
     import torch
     from ns2d import Solver, abi, initial
     from ns2d import adjoint as nadj
@@ -444,9 +447,10 @@ def adjoint_bench(stream, nsteps, rank, precision, g_ref=None, n_dirs=16):
         if n_dirs:
             best_rel = [min(rel[e][i] for e in eps_list) for i in range(n_dirs)]
             best_scaled = [min(scaled[e][i] for e in eps_list) for i in range(n_dirs)]
-            out["fd"] = {"eps": 1e-6, "directions": n_dirs, "max_rel_err": max(rel[1e-6]),
-                         "median_rel_err": float(np.median(rel[1e-6])),
-                         "max_err_over_grad_norm": max(scaled[1e-6]),
+            eps_h = min(eps_list, key=lambda e: max(rel[e]))
+            out["fd"] = {"eps": eps_h, "directions": n_dirs, "max_rel_err": max(rel[eps_h]),
+                         "median_rel_err": float(np.median(rel[eps_h])),
+                         "max_err_over_grad_norm": max(scaled[eps_h]),
                          "eps_sweep": list(eps_list),
                          "max_rel_err_by_eps": [max(rel[e]) for e in eps_list],
                          "max_rel_err_best_eps": max(best_rel),
