@@ -2,7 +2,6 @@
 // the host-side sequencing of the step kernels.  Each entry point names the
 // reference function it replaces (EndCar808/2D-Navier-Stokes, Solver/src).
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <climits>
@@ -161,43 +160,18 @@ struct TimedLaunch {
     }
 };
 
-// The driver's tensor-map encoder, through the runtime (no libcuda link).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }();
-    return fn;
-}
-
 // Tensor maps for the column passes' TMA tile copies of f[0..3], acc, state and
 // nl (see ColMaps).  Leaves h->col_maps null when a map cannot be encoded; the
 // column passes then copy per thread.
 template <typename Real>
 void build_col_maps(ns2d_handle* h) {
-    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     const int tc = col_tc(h->nx);
-    if (!enc || tc == 0) return;
     auto* m = new (std::nothrow) ColMaps;
     if (!m) return;
-    const cuuint64_t gdim[2] = {(cuuint64_t)2 * h->nyf, (cuuint64_t)h->nx};
-    const cuuint64_t gstride[1] = {(cuuint64_t)h->ldc * 2 * sizeof(Real)};
-    const cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)std::min(h->nx, 256)};
-    const cuuint32_t estride[2] = {1, 1};
-    const CUtensorMapDataType dt = sizeof(Real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    CUtensorMap* maps[7] = {&m->f[0], &m->f[1], &m->f[2], &m->f[3], &m->acc, &m->state, &m->nl};
-    void* bases[7] = {h->f[0], h->f[1], h->f[2], h->f[3], h->acc, h->state, h->nl};
-    for (int k = 0; k < 7; ++k) {
-        if (enc(maps[k], dt, 2, bases[k], gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
-            delete m;
-            return;
-        }
+    void* const bases[7] = {h->f[0], h->f[1], h->f[2], h->f[3], h->acc, h->state, h->nl};
+    if (!encode_col_maps<Real>(m, bases, h->nx, h->nyf, h->ldc, tc)) {
+        delete m;
+        return;
     }
     h->col_maps = m;
 }

@@ -63,7 +63,10 @@ struct ns2d_ensemble {
     double graph_dt = -1.0;
     int graph_col_grid = 0, graph_row_grid = 0, graph_col_var = -1, graph_row_var = -1;
     int graph_fused = -1, graph_stage_grid = 0;
-    size_t col_smem[2] = {0, 0}, row_smem[2] = {0, 0};
+    size_t col_smem[2] = {0, 0}, row_smem[2] = {0, 0}, col_tma_smem[2] = {0, 0};
+    // tensor maps of every member's arrays for the TMA column kernels,
+    // [member][block-size choice]; null when they are not used
+    ColMaps* maps = nullptr;
     int nsm = 148;
 };
 
@@ -118,6 +121,7 @@ cudaError_t ens_set_smem(ns2d_ensemble* e) {
     constexpr int TH = kEnsThreadChoices[V];
     e->col_smem[V] = EnsSmem<Real, TH>::col();
     e->row_smem[V] = EnsSmem<Real, TH>::row();
+    e->col_tma_smem[V] = EnsSmem<Real, TH>::col_tma();
     cudaError_t r = cudaSuccess;
     auto set = [&](const void* f, size_t b) {
         if (r == cudaSuccess) r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
@@ -127,16 +131,11 @@ cudaError_t ens_set_smem(ns2d_ensemble* e) {
     set((const void*)ens_col_kernel<Real, COL_FINAL, TH>, e->col_smem[V]);
     set((const void*)ens_col_kernel<Real, COL_STAGE, TH, true>, e->col_smem[V]);
     set((const void*)ens_col_kernel<Real, COL_FINAL, TH, true>, e->col_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_P1, TH, true, true>, e->col_tma_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_STAGE, TH, true, true>, e->col_tma_smem[V]);
+    set((const void*)ens_col_kernel<Real, COL_FINAL, TH, true, true>, e->col_tma_smem[V]);
     set((const void*)ens_row_kernel<Real, TH>, e->row_smem[V]);
     return r;
-}
-
-// Blocks per SM of the choice's column and row kernels.
-template <typename Real, int V>
-void ens_occupancy(const ns2d_ensemble* e, int* col_per_sm, int* row_per_sm) {
-    constexpr int TH = kEnsThreadChoices[V];
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(col_per_sm, ens_col_kernel<Real, COL_STAGE, TH>, TH, e->col_smem[V]);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(row_per_sm, ens_row_kernel<Real, TH>, TH, e->row_smem[V]);
 }
 
 // Whether the stage and final column passes of this ensemble can run the
@@ -146,20 +145,38 @@ bool ens_fast(const ns2d_ensemble* e) {
            e->p.model == NS2D_MODEL_FULL;
 }
 
-template <typename Real, int MODE, int V, bool FAST>
-void ens_launch_col_v(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
+// Blocks per SM of the choice's column and row kernels.
+template <typename Real, int V>
+void ens_occupancy(const ns2d_ensemble* e, int* col_per_sm, int* row_per_sm) {
     constexpr int TH = kEnsThreadChoices[V];
-    ens_col_kernel<Real, MODE, TH, FAST><<<e->col_grid, TH, e->col_smem[V], e->stream>>>(mb, e->col_items[V],
-                                                                                       e->n_col_items[V], st);
+    if (e->maps && ens_fast(e))
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(col_per_sm, ens_col_kernel<Real, COL_STAGE, TH, true, true>, TH,
+                                                      e->col_tma_smem[V]);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(col_per_sm, ens_col_kernel<Real, COL_STAGE, TH>, TH, e->col_smem[V]);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(row_per_sm, ens_row_kernel<Real, TH>, TH, e->row_smem[V]);
 }
 
+
+template <typename Real, int MODE, int V, bool FAST, bool TMA = false>
+void ens_launch_col_v(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
+    constexpr int TH = kEnsThreadChoices[V];
+    ens_col_kernel<Real, MODE, TH, FAST, TMA><<<e->col_grid, TH, TMA ? e->col_tma_smem[V] : e->col_smem[V], e->stream>>>(
+        mb, e->col_items[V], e->n_col_items[V], st, e->maps);
+}
+
+// The TMA column kernels run the common step (ens_fast) when the members'
+// tensor maps exist; otherwise per-thread copies.
 template <typename Real, int MODE>
 void ens_launch_col(ns2d_ensemble* e, const EnsMember<Real>* mb, const EnsStage& st) {
-    if constexpr (MODE == COL_P1) {
+    const bool fast = ens_fast(e);
+    if (fast && e->maps) {
+        if (e->col_var == 0) ens_launch_col_v<Real, MODE, 0, true, true>(e, mb, st);
+        else ens_launch_col_v<Real, MODE, 1, true, true>(e, mb, st);
+    } else if constexpr (MODE == COL_P1) {
         if (e->col_var == 0) ens_launch_col_v<Real, MODE, 0, false>(e, mb, st);
         else ens_launch_col_v<Real, MODE, 1, false>(e, mb, st);
     } else {
-        const bool fast = ens_fast(e);
         if (e->col_var == 0) {
             if (fast) ens_launch_col_v<Real, MODE, 0, true>(e, mb, st);
             else ens_launch_col_v<Real, MODE, 0, false>(e, mb, st);
@@ -272,6 +289,24 @@ ns2d_status create_t(ns2d_ensemble* e) {
     }
     ECK(e, alloc(sizeof(EnsMember<Real>) * e->n, &e->members));
     ECK(e, cudaMemcpyAsync(e->members, hm.data(), sizeof(EnsMember<Real>) * e->n, cudaMemcpyHostToDevice, e->stream));
+    if (ens_fast(e)) {
+        // tensor maps of each member's arrays for both block-size choices
+        std::vector<ColMaps> hmaps(2 * (size_t)e->n);
+        bool ok = true;
+        for (int m = 0; m < e->n && ok; ++m) {
+            const ColArgs<Real>& a = hm[m].col;
+            void* const bases[7] = {a.f0, a.f1, a.f2, a.f3, a.acc, a.state, (void*)a.src};
+            for (int v = 0; v < 2 && ok; ++v)
+                ok = encode_col_maps<Real>(&hmaps[2 * m + v], bases, e->sizes[m], a.nyf, a.ldc, ens_col_tc(e->sizes[m], v));
+        }
+        if (ok) {
+            void* dm = nullptr;
+            ECK(e, alloc(sizeof(ColMaps) * hmaps.size(), &dm));
+            ECK(e, cudaMemcpyAsync(dm, hmaps.data(), sizeof(ColMaps) * hmaps.size(), cudaMemcpyHostToDevice, e->stream));
+            ECK(e, cudaStreamSynchronize(e->stream));
+            e->maps = (ColMaps*)dm;
+        }
+    }
     ECK(e, alloc(sizeof(double2) * io_elems, (void**)&e->io));
     ECK(e, alloc(sizeof(int) * 4, (void**)&e->status));
     int nspect_max = 0;
@@ -505,6 +540,7 @@ ns2d_status check_impl(ns2d_ensemble* e) {
     ECK(e, cudaStreamSynchronize(e->stream));
     if (st[0] & 1) return efail(e, NS2D_ERR_BLOWUP, "non-finite vorticity in an ensemble member");
     if (st[0] & 4) return efail(e, NS2D_ERR_CUDA, "a per-stage launch waited past its bound for a member's tasks");
+    if (st[0] & 8) return efail(e, NS2D_ERR_CUDA, "a column pass waited past its bound for its tile loads");
     return NS2D_OK;
 }
 

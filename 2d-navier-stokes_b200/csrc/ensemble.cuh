@@ -83,25 +83,36 @@ struct EnsMinBlocks {
     static constexpr int value = sizeof(Real) == 4 ? 512 / THREADS : 256 / THREADS;
 };
 
-template <typename Real, int MODE, int THREADS, bool FAST = false>
+// TMA (with FAST): the tiles move by TMA copies through maps[2 m + v], the
+// tensor maps of member m for this block size (v = 0 for kEnsThreadChoices[0],
+// 1 for the other); shared memory EnsSmem::col_tma().  A tile whose loads do
+// not land within their bound stops the block (status bit 8).
+template <typename Real, int MODE, int THREADS, bool FAST = false, bool TMA = false>
 __global__ void __launch_bounds__(THREADS, (EnsMinBlocks<Real, THREADS>::value)) ens_col_kernel(const EnsMember<Real>* __restrict__ members,
-                                                      const EnsItem* __restrict__ items, int nitems, EnsStage st) {
+                                                      const EnsItem* __restrict__ items, int nitems, EnsStage st,
+                                                      const ColMaps* __restrict__ maps) {
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(st.status)) return;
+    unsigned char* sm = smraw;
+    if constexpr (TMA) sm = smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
+    constexpr int VI = THREADS == kEnsThreadChoices[0] ? 0 : 1;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const EnsItem item = items[it];
         const EnsMember<Real>& mb = members[item.member];
         ColArgs<Real> a = mb.col;
         ens_apply_stage(a, mb, st);
+        const ColMaps* mp = TMA ? maps + 2 * item.member + VI : nullptr;
+        bool go = true;
         switch (mb.n) {
-#define NS2D_ENS_COL(NN)                                                                  \
-    case NN:                                                                              \
-        col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE, FAST>(a, item.tile, smraw);   \
+#define NS2D_ENS_COL(NN)                                                                           \
+    case NN:                                                                                       \
+        go = col_body<Real, NN, EnsShape<NN, THREADS>::TC, MODE, FAST, TMA>(a, item.tile, sm, mp); \
         break;
             NS2D_ENS_SIZES(NS2D_ENS_COL)
 #undef NS2D_ENS_COL
             default: break;
         }
+        if (!go) return;
     }
 }
 
@@ -249,6 +260,16 @@ struct EnsSmem {
         NS2D_ENS_SIZES(NS2D_ENS_RS)
 #undef NS2D_ENS_RS
         return m;
+    }
+    // the TMA column kernels: three exchange-sized regions and 1 KB of alignment
+    static size_t col_tma() {
+        size_t m = 0;
+#define NS2D_ENS_CT(NN)                                                                           \
+    m = m > ColSmem<Real, NN, EnsShape<NN, THREADS>::TC>::bytes_tma() ? m                          \
+                                                                      : ColSmem<Real, NN, EnsShape<NN, THREADS>::TC>::bytes_tma();
+        NS2D_ENS_SIZES(NS2D_ENS_CT)
+#undef NS2D_ENS_CT
+        return m + 1024;
     }
     static size_t stage() { return col() > row() ? col() : row(); }
 };

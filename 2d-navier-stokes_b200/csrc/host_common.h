@@ -1,6 +1,11 @@
 // host_common.h -- host-side rules shared by the single-trajectory handle and
-// the ensemble: operator-branch selection and exponent handling.
+// the ensemble: operator-branch selection, exponent handling and the tensor
+// maps of the column passes' TMA tile copies.
 #pragma once
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -38,5 +43,41 @@ inline LinOp make_lin_params(const ns2d_params& p, int branch) {
 }
 
 inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// The driver's tensor-map encoder, through the runtime (no libcuda link).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The ColMaps of one field set, bases = {f0, f1, f2, f3, acc, state, nl}, each
+// nx rows of ldc complex (nyf used) with column tiles of tc columns: boxes of
+// (2 tc reals, min(nx, 256) rows).  False when the encoder is missing or
+// rejects a map.
+template <typename Real>
+inline bool encode_col_maps(ColMaps* m, void* const bases[7], int nx, int nyf, int ldc, int tc) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || tc <= 0) return false;
+    const cuuint64_t gdim[2] = {(cuuint64_t)2 * nyf, (cuuint64_t)nx};
+    const cuuint64_t gstride[1] = {(cuuint64_t)ldc * 2 * sizeof(Real)};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)std::min(nx, 256)};
+    const cuuint32_t estride[2] = {1, 1};
+    const CUtensorMapDataType dt = sizeof(Real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap* maps[7] = {&m->f[0], &m->f[1], &m->f[2], &m->f[3], &m->acc, &m->state, &m->nl};
+    for (int k = 0; k < 7; ++k) {
+        if (enc(maps[k], dt, 2, bases[k], gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
 
 }  // namespace ns2d

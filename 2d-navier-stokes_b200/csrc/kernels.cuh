@@ -194,6 +194,11 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
+// Invalidate `bar` (every thread is past its last wait on it) so that the
+// same shared memory can hold a fresh barrier for the next tile.
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
 // Bounded wait for phase 0 of `bar`: false if the loads have not landed after
 // 2^22 polls (each poll may suspend the thread for a while in hardware).
 __device__ __forceinline__ bool mbar_wait0(unsigned long long* bar) {
@@ -412,10 +417,12 @@ __device__ __forceinline__ void derived_ifft_tma(typename Cx<Real>::T* pre0, typ
 // a.acc) arrive by TMA tile loads and its outputs (the x-space fields, the
 // accumulator, the final state) leave by bulk-async tile stores, through `maps`
 // (which must describe those arrays), instead of per-thread copies; smraw
-// 1024-byte aligned.  A load that does not land within its bound sets status
-// bit 8 and the block returns.
+// 1024-byte aligned.  Its mbarriers are invalidated once used, so a persistent
+// caller can run the body again on the same shared memory.  A load that does
+// not land within its bound sets status bit 8 and the body returns false (the
+// block must stop); otherwise it returns true.
 template <typename Real, int N, int TC, int MODE, bool FAST = false, bool TMA = false>
-__device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw,
+__device__ __forceinline__ bool col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw,
                                          const ColMaps* maps = nullptr) {
     static_assert(!TMA || (FAST && MODE != COL_RHS), "TMA copies: FAST P1, STAGE and FINAL only");
     using C = typename Cx<Real>::T;
@@ -449,8 +456,9 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                     atomicOr(a.status, 8);
                     mbar_wait0(&bar_in);
                 }
-                return;
+                return false;
             }
+            if (threadIdx.x == 0) mbar_inval(&bar_in);
         } else {
             const C* __restrict__ src = a.src;
 #pragma unroll
@@ -495,8 +503,9 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                     atomicOr(a.status, 8);
                     mbar_wait0(&bar_tile[1]);
                 }
-                return;
+                return false;
             }
+            if (threadIdx.x == 0) mbar_inval(&bar_tile[0]);
         } else {
 #pragma unroll
             for (int m = 0; m < E; ++m) {
@@ -537,8 +546,9 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             const bool late = !mbar_wait0(&bar_tile[1]);
             if (__syncthreads_or(late)) {
                 if (threadIdx.x == 0) atomicOr(a.status, 8);
-                return;
+                return false;
             }
+            if (threadIdx.x == 0) mbar_inval(&bar_tile[1]);
         } else if constexpr (need_state) {
             cp_async_wait_all();
         }
@@ -678,7 +688,7 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
                 if constexpr (TMA) {
                     if (threadIdx.x == 0) bulk_wait_all();
                 }
-                return;
+                return true;
             }
             // SystemCheck (solver.c:2301-2326) without a transform: max|w(x)| is
             // bounded by sum|w_hat|/(Nx Ny) over the full spectrum.  Status bit 1:
@@ -707,13 +717,14 @@ __device__ __forceinline__ void col_body(const ColArgs<Real>& a, int tile, unsig
             if constexpr (TMA) {
                 if (threadIdx.x == 0) bulk_wait_all();
             }
-            return;
+            return true;
         }
-        if constexpr (MODE == COL_RHS) return;
+        if constexpr (MODE == COL_RHS) return true;
     }
 
     if constexpr (TMA) derived_ifft_tma<Real, N, TC>(pre0, sm, maps, tile, ky, t, c, seed, MODE == COL_STAGE);
     else derived_ifft<Real, N, TC>(pre0, sm, a.f0, a.f1, a.f2, a.f3, ldc, ky, valid, t, c, seed);
+    return true;
 }
 
 // Column pass of one field.  Grid: ceil(nyf / TC) blocks; block: T * TC threads.
