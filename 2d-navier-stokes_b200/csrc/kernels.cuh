@@ -853,10 +853,12 @@ __device__ __forceinline__ void row_body(const RowArgs<Real>& a, int rblock, uns
     // complex sequence z[j] = n[2j] + i n[2j+1] and splits the result,
     //   X[k] = (Z[k] + conj Z[N/2-k])/2 + W^k (Z[k] - conj Z[N/2-k])/(2i),
     // W = exp(-2 pi i / N), k = 0..N/2 (Z periodic in N/2): both teams work and
-    // only team barriers are needed.  Where the N/2 plan has another team width
-    // the rows of a pair share one packed N-point transform instead.
+    // only team barriers are needed (below a warp, both teams of a pair would
+    // otherwise each run the pair's whole packed transform).  Where the N/2 plan
+    // has another team width the rows of a pair share one packed N-point
+    // transform instead.
     constexpr int NH = N / 2;
-    constexpr bool HALF = (T >= 32) && (half_plan_width<N>() == T);
+    constexpr bool HALF = half_plan_width<N>() == T;
     if constexpr (HALF) {
         constexpr int EH = NH / T;
         using TLH = TeamLayout<NH>;
