@@ -214,7 +214,9 @@ ns2d_status ns2d_rk4_step_host(ns2d_handle* h, double* w_hat, double dt);
    waiting.  Failures detected on the device (SystemCheck) are reported by the
    next ns2d_check. */
 ns2d_status ns2d_step_async(ns2d_handle* h, int32_t nsteps, double dt);
-/* Wait for queued work and apply SystemCheck (solver.c:2301) to it. */
+/* Wait for queued work and apply SystemCheck (solver.c:2301) to it.  Also
+   returns NS2D_ERR_CUDA when a column pass's bounded wait for its own TMA tile
+   copies ran out (no counterpart in the reference). */
 ns2d_status ns2d_check(ns2d_handle* h);
 
 /* ApplyDealiasing (solver.c:1039) on a host array of array_dim interleaved
