@@ -165,6 +165,7 @@ struct TimedLaunch {
 // column passes then copy per thread.
 template <typename Real>
 void build_col_maps(ns2d_handle* h) {
+    if (!tma_copies_enabled()) return;
     const int tc = col_tc(h->nx);
     auto* m = new (std::nothrow) ColMaps;
     if (!m) return;

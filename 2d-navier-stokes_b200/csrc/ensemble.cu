@@ -289,7 +289,7 @@ ns2d_status create_t(ns2d_ensemble* e) {
     }
     ECK(e, alloc(sizeof(EnsMember<Real>) * e->n, &e->members));
     ECK(e, cudaMemcpyAsync(e->members, hm.data(), sizeof(EnsMember<Real>) * e->n, cudaMemcpyHostToDevice, e->stream));
-    if (ens_fast(e)) {
+    if (ens_fast(e) && tma_copies_enabled()) {
         // tensor maps of each member's arrays for both block-size choices
         std::vector<ColMaps> hmaps(2 * (size_t)e->n);
         bool ok = true;

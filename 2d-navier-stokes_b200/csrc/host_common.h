@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 
 #include "../../include/ns2d.h"
 #include "kernels.cuh"
@@ -43,6 +44,15 @@ inline LinOp make_lin_params(const ns2d_params& p, int branch) {
 }
 
 inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// Whether the column passes may move their tiles by TMA copies: yes unless the
+// environment variable NS2D_DISABLE_TMA is set to a value other than "0" when
+// a handle or ensemble is created (the per-thread copies give the same
+// results to rounding; the switch exists to compare the two and as a fallback).
+inline bool tma_copies_enabled() {
+    const char* v = std::getenv("NS2D_DISABLE_TMA");
+    return !(v && v[0] && !(v[0] == '0' && v[1] == 0));
+}
 
 // The driver's tensor-map encoder, through the runtime (no libcuda link).
 inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
