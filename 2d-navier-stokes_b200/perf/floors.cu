@@ -10,7 +10,10 @@
 //      warm (data left by the previous launch, as inside a step) and after a
 //      256 MiB write that evicts it (as at the start of a step);
 //   2. the compute throughput of the FFT engine (fft.cuh) on 1024-point FP64
-//      transforms held in registers: eight transforms per load and store.
+//      transforms held in registers: eight transforms per load and store; and
+//      the same for the warp-per-transform engine (wfft.cuh: two radix-32
+//      stages, one shared-memory transpose), the alternative it was measured
+//      against.
 //
 // Build and run:  make -C 2d-navier-stokes_b200 floors && 2d-navier-stokes_b200/bin/ns2d_floors
 #include <cuda_runtime.h>
@@ -21,6 +24,7 @@
 #include <vector>
 
 #include "../csrc/fft.cuh"
+#include "../csrc/wfft.cuh"
 
 using namespace ns2d;
 
@@ -73,6 +77,26 @@ __global__ void __launch_bounds__(128) fft_kernel(const double2* in, double2* ou
     for (int r = 0; r < REPS; ++r) fft_batched<kN, -1, 1>(v, pol, seed, t);
 #pragma unroll
     for (int m = 0; m < 16; ++m) out[(size_t)row * kN + t + 64 * m] = v[0][m];
+}
+
+// REPS in-register 1024-point transforms per row by the warp engine: one warp
+// per row (lane t holds x[t + 32 m]), four rows per 128-thread block, a private
+// 32 x 33 transpose tile per warp.
+template <int REPS>
+__global__ void __launch_bounds__(128) wfft_kernel(const double2* in, double2* out, const double2* tw, int rows) {
+    extern __shared__ __align__(16) double2 wsm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int row = blockIdx.x * 4 + w;
+    if (row >= rows) return;
+    double2* tile = wsm + w * WfftTile<double2>::ELEMS;
+    const double2 w1 = __ldg(tw + lane);
+    double2 v[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) v[m] = in[(size_t)row * kN + lane + 32 * m];
+#pragma unroll 1
+    for (int r = 0; r < REPS; ++r) wfft1024<-1>(v, tile, w1, lane);
+#pragma unroll
+    for (int m = 0; m < 32; ++m) out[(size_t)row * kN + lane + 32 * m] = v[m];
 }
 
 struct Timer {
@@ -180,5 +204,34 @@ int main() {
     std::printf("\nFFT engine: 1024-point FP64 transform, in registers: %.2f ns per transform on the device\n", ns_per);
     std::printf("  (%d rows, 64-thread teams; the RK4 step needs about 20,500 such transforms: %.1f us)\n", rows,
                 ns_per * 20500.0 * 1e-3);
+
+    // the warp-per-transform engine, same method
+    const size_t wsmem = 4 * WfftTile<double2>::bytes();
+    FCK(cudaFuncSetAttribute((const void*)wfft_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
+    FCK(cudaFuncSetAttribute((const void*)wfft_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
+    float wms8 = 0, wms1 = 0;
+    for (int k = 0; k < 2; ++k) {
+        wfft_kernel<8><<<rows / 4, 128, wsmem>>>(in, out, tw, rows);
+        wfft_kernel<1><<<rows / 4, 128, wsmem>>>(in, out, tw, rows);
+    }
+    FCK(cudaDeviceSynchronize());
+    for (int k = 0; k < 20; ++k) {
+        float ms;
+        FCK(cudaEventRecord(tm.a));
+        wfft_kernel<8><<<rows / 4, 128, wsmem>>>(in, out, tw, rows);
+        FCK(cudaEventRecord(tm.b));
+        FCK(cudaEventSynchronize(tm.b));
+        FCK(cudaEventElapsedTime(&ms, tm.a, tm.b));
+        wms8 += ms;
+        FCK(cudaEventRecord(tm.a));
+        wfft_kernel<1><<<rows / 4, 128, wsmem>>>(in, out, tw, rows);
+        FCK(cudaEventRecord(tm.b));
+        FCK(cudaEventSynchronize(tm.b));
+        FCK(cudaEventElapsedTime(&ms, tm.a, tm.b));
+        wms1 += ms;
+    }
+    FCK(cudaGetLastError());
+    const double wns_per = (wms8 - wms1) / 20.0 * 1e6 / (7.0 * rows);
+    std::printf("Warp engine (wfft.cuh): %.2f ns per transform on the device (one warp per row)\n", wns_per);
     return 0;
 }
