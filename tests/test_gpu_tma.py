@@ -41,10 +41,11 @@ def _steps(params, w0, nsteps, dt, tma):
         s.close()
 
 
-@pytest.mark.parametrize("n,precision", [(256, abi.FP64), (512, abi.FP32), (1024, abi.FP32)])
+@pytest.mark.parametrize("n,precision", [(16, abi.FP64), (32, abi.FP32), (256, abi.FP64), (512, abi.FP32),
+                                         (1024, abi.FP32), (2048, abi.FP64)])
 def test_single_field_tma_equals_per_thread_copies(n, precision):
     p = abi.default_params(nx=n, ny=n, nu=1e-3, dt=1e-3, precision=precision)
-    w0 = initial.decaying(n, seed=11, k0=4.0 * n / 128.0, dealias="2/3")
+    w0 = initial.decaying(n, seed=11, k0=max(2.0, 4.0 * n / 128.0), dealias="2/3")
     a = _steps(p, w0, 6, 1e-3, True)
     b = _steps(p, w0, 6, 1e-3, False)
     err = rel_err(a, b)
