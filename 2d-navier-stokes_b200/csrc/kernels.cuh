@@ -352,14 +352,18 @@ __device__ __forceinline__ void derived_ifft(const typename Cx<Real>::T* pre0, t
 }
 
 // derived_ifft with TMA stores.  The three shared regions B0 = sm, B1 = sm +
-// STRIDE and B2 = pre0 (sized as an exchange buffer in this form) rotate: the
-// first pair transforms in (B0, B1) and is staged there, each field stored by
-// its own bulk-async group; the second pair's spectra are formed from B2 (the
-// stage input), which is then free, so it transforms in (B2, B0) as soon as
-// the first field's store has read B0, while the second field still drains
-// from B1.  pending: a store issued before this call still reads B1 (the
-// accumulator).  Thread 0 returns once all stores have completed.
-template <typename Real, int N, int TC>
+// STRIDE and B2 = pre0 (sized as an exchange buffer in this form) rotate.  The
+// first pair (U, V) transforms batched in (B0, B1) and is staged there, each
+// field stored by its own bulk-async group.  The second pair (WX, WY) runs as
+// two single transforms: WX in B2 (the stage input, free once both spectra are
+// formed), WY in B0 as soon as the U store has read it; so the first pair's
+// stores drain under the second pair's transforms and only WY's store is left
+// to drain at the end.  Without SPLIT the second pair transforms batched in
+// (B2, B0) instead (a persistent caller's next tile overlaps the drain, and the
+// batched pair keeps the transforms' ILP).  pending: a store issued before
+// this call still reads B1 (the accumulator).  Thread 0 returns once all
+// stores have completed.
+template <typename Real, int N, int TC, bool SPLIT>
 __device__ __forceinline__ void derived_ifft_tma(typename Cx<Real>::T* pre0, typename Cx<Real>::T* sm,
                                                  const ColMaps* maps, int tile, int ky, int t, int c,
                                                  TwSeed<typename Cx<Real>::T> seed, bool pending) {
@@ -371,39 +375,96 @@ __device__ __forceinline__ void derived_ifft_tma(typename Cx<Real>::T* pre0, typ
     C* const B0 = sm;
     C* const B1 = sm + STRIDE;
     C* const B2 = pre0;
+    if constexpr (!SPLIT) {
+        // both pairs batched, one copy of the transform code: (B0, B1), then (B2, B0)
 #pragma unroll 1
-    for (int fp = 0; fp < 4; fp += 2) {
+        for (int fp = 0; fp < 4; fp += 2) {
+            C v[2][E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int i = t + T * m;
+                derived_pair(fp, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
+            }
+            // first pair: the accumulator store (if any) must have read B1;
+            // second pair: the first pair's first field must have left B0 (at
+            // most its second group still pending), and every thread has read B2
+            if (fp == 0 ? pending : true) {
+                if (threadIdx.x == 0) {
+                    if (fp == 0) bulk_wait_read_all();
+                    else asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+                }
+                __syncthreads();
+            }
+            C* const Pa = fp == 0 ? B0 : B2;
+            C* const Pb = fp == 0 ? B1 : B0;
+            fft_batched<N, +1, 2>(v, IlvPairPolicy<N, TC, C>{Pa, Pb, c}, seed, t);
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                Pa[(t + T * m) * TC + c] = v[0][m];
+                Pb[(t + T * m) * TC + c] = v[1][m];
+            }
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tma_store_tile<C, N, TC>(&maps->f[fp], tile, Pa);
+                bulk_commit();
+                tma_store_tile<C, N, TC>(&maps->f[fp + 1], tile, Pb);
+                bulk_commit();
+            }
+        }
+    } else {
+        {
+            C v[2][E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int i = t + T * m;
+                derived_pair(0, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
+            }
+            if (pending) {  // the accumulator store must have read B1
+                if (threadIdx.x == 0) bulk_wait_read_all();
+                __syncthreads();
+            }
+            fft_batched<N, +1, 2>(v, IlvPairPolicy<N, TC, C>{B0, B1, c}, seed, t);
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                B0[(t + T * m) * TC + c] = v[0][m];
+                B1[(t + T * m) * TC + c] = v[1][m];
+            }
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tma_store_tile<C, N, TC>(&maps->f[0], tile, B0);
+                bulk_commit();
+                tma_store_tile<C, N, TC>(&maps->f[1], tile, B1);
+                bulk_commit();
+            }
+        }
         C v[2][E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int i = t + T * m;
-            derived_pair(fp, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
+            derived_pair(2, kx_of<Real, N, T>(m, t, tr), kyr, pre0[i * TC + c], v[0][m], v[1][m]);
         }
-        // first pair: the accumulator store (if any) must have read B1;
-        // second pair: the first pair's first field must have left B0 (at
-        // most its second group still pending), and every thread has read B2
-        if (fp == 0 ? pending : true) {
-            if (threadIdx.x == 0) {
-                if (fp == 0) bulk_wait_read_all();
-                else asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+        __syncthreads();  // every thread has read B2
+#pragma unroll 1
+        for (int b = 0; b < 2; ++b) {
+            C* const P = b == 0 ? B2 : B0;
+            if (b == 1) {  // the U store (the oldest group) must have read B0
+                if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 2;\n" ::: "memory");
+                __syncthreads();
             }
-            __syncthreads();
-        }
-        C* const Pa = fp == 0 ? B0 : B2;
-        C* const Pb = fp == 0 ? B1 : B0;
-        fft_batched<N, +1, 2>(v, IlvPairPolicy<N, TC, C>{Pa, Pb, c}, seed, t);
+            C u[1][E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            Pa[(t + T * m) * TC + c] = v[0][m];
-            Pb[(t + T * m) * TC + c] = v[1][m];
-        }
-        fence_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            tma_store_tile<C, N, TC>(&maps->f[fp], tile, Pa);
-            bulk_commit();
-            tma_store_tile<C, N, TC>(&maps->f[fp + 1], tile, Pb);
-            bulk_commit();
+            for (int m = 0; m < E; ++m) u[0][m] = b == 0 ? v[0][m] : v[1][m];
+            fft_batched<N, +1, 1>(u, IlvPairPolicy<N, TC, C>{P, P, c}, seed, t);
+#pragma unroll
+            for (int m = 0; m < E; ++m) P[(t + T * m) * TC + c] = u[0][m];
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tma_store_tile<C, N, TC>(&maps->f[2 + b], tile, P);
+                bulk_commit();
+            }
         }
     }
     if (threadIdx.x == 0) bulk_wait_all();
@@ -417,11 +478,12 @@ __device__ __forceinline__ void derived_ifft_tma(typename Cx<Real>::T* pre0, typ
 // a.acc) arrive by TMA tile loads and its outputs (the x-space fields, the
 // accumulator, the final state) leave by bulk-async tile stores, through `maps`
 // (which must describe those arrays), instead of per-thread copies; smraw
-// 1024-byte aligned.  Its mbarriers are invalidated once used, so a persistent
+// 1024-byte aligned; SPLIT: the last inverse pair as two single transforms
+// (derived_ifft_tma).  Its mbarriers are invalidated once used, so a persistent
 // caller can run the body again on the same shared memory.  A load that does
 // not land within its bound sets status bit 8 and the body returns false (the
 // block must stop); otherwise it returns true.
-template <typename Real, int N, int TC, int MODE, bool FAST = false, bool TMA = false>
+template <typename Real, int N, int TC, int MODE, bool FAST = false, bool TMA = false, bool SPLIT = false>
 __device__ __forceinline__ bool col_body(const ColArgs<Real>& a, int tile, unsigned char* smraw,
                                          const ColMaps* maps = nullptr) {
     static_assert(!TMA || (FAST && MODE != COL_RHS), "TMA copies: FAST P1, STAGE and FINAL only");
@@ -722,7 +784,7 @@ __device__ __forceinline__ bool col_body(const ColArgs<Real>& a, int tile, unsig
         if constexpr (MODE == COL_RHS) return true;
     }
 
-    if constexpr (TMA) derived_ifft_tma<Real, N, TC>(pre0, sm, maps, tile, ky, t, c, seed, MODE == COL_STAGE);
+    if constexpr (TMA) derived_ifft_tma<Real, N, TC, SPLIT>(pre0, sm, maps, tile, ky, t, c, seed, MODE == COL_STAGE);
     else derived_ifft<Real, N, TC>(pre0, sm, a.f0, a.f1, a.f2, a.f3, ldc, ky, valid, t, c, seed);
     return true;
 }
@@ -745,7 +807,7 @@ __global__ void __launch_bounds__(Plan<N>::T * TC) col_tma_kernel(ColArgs<Real> 
     extern __shared__ __align__(16) unsigned char smraw[];
     if (block_should_exit(a.status)) return;
     unsigned char* sm = smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
-    col_body<Real, N, TC, MODE, true, true>(a, blockIdx.x, sm, &maps);
+    col_body<Real, N, TC, MODE, true, true, true>(a, blockIdx.x, sm, &maps);
 }
 
 // Whether a stage or final column pass can run the FAST epilogue.
