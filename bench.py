@@ -17,6 +17,9 @@ advances its own trajectory (replicas: the path has no exchange step), so
   e2e     ns2d_rk4_step_host: the reference-facing RK4Step contract with the
           state in pinned host memory, copied in and out every step (wall
           clock per step, L2 flushed between steps).
+  roofline  the dominant kernel class against the measured HBM bandwidth
+          (algorithmic bytes per launch over the scaled event time);
+          roofline_by_kernel gives the same for every pass class.
   --impl reference   the reference's own CPU solver (Solver/src built by
           oracle/Makefile; FFTW replaced by the oracle's FFT) on the host cores.
 """
@@ -616,6 +619,15 @@ def run_gpu(args, rank, world, local_rank):
     achieved = per_launch_bytes / (avg_ms * 1e-3) / 1e9
     step_ms = ms_max / args.steps
     model_gbs = MODEL_BYTES_PER_STEP * S_BYTES / (step_ms * 1e-3) / 1e9
+    # the same figures for every pass class of the step (the dominant one is `roofline`)
+    by_kernel = {}
+    for k in range(4):
+        if kn[k]:
+            kb = CLASS_BYTES_PER_LAUNCH[k] * S_BYTES
+            kms_avg = kms_scaled[k] / kn[k]
+            ka = kb / (kms_avg * 1e-3) / 1e9
+            by_kernel[CLASS_NAMES[k]] = {"achieved": ka, "frac": ka / peak, "algorithmic_bytes_per_launch": kb,
+                                         "avg_launch_ms": kms_avg, "traffic": ncu_traffic(k)}
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -629,6 +641,7 @@ def run_gpu(args, rank, world, local_rank):
                      "avg_launch_ms": avg_ms},
         "step_roofline": {"model_bytes_per_step": MODEL_BYTES_PER_STEP * S_BYTES, "achieved": model_gbs,
                           "frac": model_gbs / peak, "unit": "GB/s"},
+        "roofline_by_kernel": by_kernel,
         "kernels": {CLASS_NAMES[k]: {"ms_total": float(kms_scaled[k]), "ms_total_instrumented": float(kms[k]),
                                      "launches": int(kn[k]),
                                      "share": float(kms[k] / max(kms.sum(), 1e-30))} for k in range(5) if kn[k]},
