@@ -562,7 +562,9 @@ __device__ __forceinline__ bool col_body(const ColArgs<Real>& a, int tile, unsig
             // every thread has its input before the transform reuses the buffer
             if (__syncthreads_or(late)) {
                 if (threadIdx.x == 0) {
+                    // once more, bounded, for the copies still in flight
                     atomicOr(a.status, 8);
+                    mbar_wait0(&bar_tile[0]);
                     mbar_wait0(&bar_tile[1]);
                 }
                 return false;
@@ -607,7 +609,10 @@ __device__ __forceinline__ bool col_body(const ColArgs<Real>& a, int tile, unsig
         if constexpr (TMA) {
             const bool late = !mbar_wait0(&bar_tile[1]);
             if (__syncthreads_or(late)) {
-                if (threadIdx.x == 0) atomicOr(a.status, 8);
+                if (threadIdx.x == 0) {
+                    atomicOr(a.status, 8);
+                    mbar_wait0(&bar_tile[1]);  // once more, bounded, for the copies still in flight
+                }
                 return false;
             }
             if (threadIdx.x == 0) mbar_inval(&bar_tile[1]);
