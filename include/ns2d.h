@@ -134,6 +134,12 @@ typedef struct ns2d_handle ns2d_handle;
    flux diagnostics on, all reference quirks on, FP64. */
 ns2d_status ns2d_params_default(ns2d_params* p);
 
+/* Allocates the handle's device arrays on p->device and encodes the tensor
+   maps its column passes use for TMA tile copies.  With the environment
+   variable NS2D_DISABLE_TMA set (to anything but "0") when the handle is
+   created, or when the driver offers no tensor-map encoder, those passes copy
+   per thread instead: the same results to rounding, slower.  (No counterpart
+   in the reference, which allocates in AllocateMemory, solver.c:2603.) */
 ns2d_status ns2d_create(const ns2d_params* p, ns2d_handle** out);
 ns2d_status ns2d_destroy(ns2d_handle* h);
 const char* ns2d_last_error(const ns2d_handle* h);
